@@ -1,0 +1,174 @@
+/*
+ * vortrace_b200.h -- C ABI of libvortrace_b200.so, the B200 (sm_100a)
+ * implementation of vortrace's exact ray walk through Voronoi meshes.
+ *
+ * The library replaces the reference's pybind11 module ``Cvortrace``
+ * (src/bindings.cpp:71-326) for the projection path.  Every entry point
+ * below names the reference interface it stands in for.  Conventions:
+ *   - plain pointers and sizes, no C++ or framework types;
+ *   - inputs are float64, C-contiguous, and copied by the callee unless the
+ *     entry point says "device" (then they are device pointers that stay
+ *     owned by the caller);
+ *   - every call returns a status code: VT_OK, VT_ERR_INVALID (the
+ *     reference's std::invalid_argument, i.e. Python ValueError) or another
+ *     code (the reference's std::runtime_error, i.e. Python RuntimeError);
+ *     the message is available from vt_last_error() on the calling thread;
+ *   - a vt_cloud handle owns its device memory and one CUDA stream; calls on
+ *     one handle are serialised by an internal mutex.
+ */
+#ifndef VORTRACE_B200_H
+#define VORTRACE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VT_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define VT_OK 0
+#define VT_ERR_INVALID 1   /* reference: std::invalid_argument -> ValueError */
+#define VT_ERR_RUNTIME 2   /* reference: std::runtime_error -> RuntimeError  */
+#define VT_ERR_CUDA 3      /* a CUDA call failed (no reference counterpart)  */
+#define VT_ERR_NOMEM 4     /* host or device allocation failed               */
+/* per-ray walk failures, one per throw site of the reference's Ray::walk   */
+#define VT_ERR_MAX_ITER 10     /* src/ray.cpp:260-261 MAX_ITERATIONS           */
+#define VT_ERR_SPLIT_BOUNDS 11 /* src/ray.cpp:282-289 split outside segment    */
+#define VT_ERR_BINSEARCH 12    /* src/ray.cpp:125-126 bisection no convergence */
+#define VT_ERR_PERTURB 13      /* src/ray.cpp:182-184 perturbation exhausted   */
+#define VT_ERR_KNN_EXPAND 14   /* src/ray.cpp:331-336 100-NN classification   */
+#define VT_ERR_STACK 15        /* pending-point stack above VT_PARAM_STACK_CAP
+                                  (the reference's list is heap-grown)         */
+
+/* ---- reduction modes: include/mytypes.hpp:14 (ReductionMode) ----------- */
+#define VT_REDUCE_SUM 0
+#define VT_REDUCE_MAX 1
+#define VT_REDUCE_MIN 2
+#define VT_REDUCE_VOLUME 3
+
+/* ---- walk kernels ------------------------------------------------------ */
+#define VT_KERNEL_AUTO 0        /* the batched guarded-FP32 kernel          */
+#define VT_KERNEL_PLAIN_FP64 1  /* one ray per thread, full-FP64 k-NN       */
+#define VT_KERNEL_BATCHED 2     /* persistent work queue, guarded-FP32 k-NN */
+#define VT_KERNEL_BATCHED_FP64 3 /* persistent work queue, FP64 k-NN        */
+
+/* ---- tunable parameters (vt_cloud_set_param) --------------------------- */
+#define VT_PARAM_MAX_ITERATIONS 1 /* src/ray.cpp:10, default 100000           */
+#define VT_PARAM_STACK_CAP 2      /* pending ray points per ray, default 4096  */
+#define VT_PARAM_BLOCK_SIZE 3     /* threads per block of the batched kernel   */
+#define VT_PARAM_SMEM_LEVELS 4    /* tree levels staged in shared memory       */
+#define VT_PARAM_BLOCKS_PER_SM 5  /* resident blocks per SM (0 = occupancy)    */
+#define VT_PARAM_LEAF_SIZE 6      /* max points per tree leaf (before build)   */
+
+typedef struct vt_cloud vt_cloud;
+typedef struct vt_segments vt_segments;
+
+typedef struct {
+  uint64_t npart;      /* points after filtering (PointCloud::get_npart)   */
+  uint64_t nfields;    /* fields per point (get_nfields)                    */
+  double pad;          /* filtering pad (get_pad)                           */
+  double subbox[6];    /* [xmin,xmax,ymin,ymax,zmin,zmax] (get_subbox)     */
+  int32_t valid_rgba;  /* get_valid_rgba                                    */
+  int32_t tree_built;  /* get_tree_built                                    */
+  int32_t periodic;    /* get_periodic                                      */
+  int32_t tree_depth;  /* internal levels of the implicit tree              */
+  uint64_t tree_leaves;
+  double tree_build_ms;
+  uint64_t device_bytes; /* device memory held by the handle                */
+} vt_cloud_info;
+
+typedef struct {
+  uint64_t rays;          /* rays walked                                      */
+  uint64_t crossings;     /* segments (cell crossings) produced               */
+  uint64_t queries;       /* k-NN queries issued                              */
+  uint64_t fp64_resolves; /* guarded-FP32 queries re-resolved fully in FP64  */
+  uint64_t slow_rays;     /* rays finished by the degenerate-geometry kernel */
+  uint64_t max_stack;     /* deepest pending-point stack seen                */
+  double walk_ms;         /* device time of the walk launch(es)               */
+} vt_stats;
+
+/* ---- library ----------------------------------------------------------- */
+int vt_abi_version(void);
+/* Thread-local message of the last failing call on this thread. */
+const char *vt_last_error(void);
+/* vortrace::verbose (include/mytypes.hpp:17; src/bindings.cpp:91-95) */
+void vt_set_verbose(int verbose);
+int vt_get_verbose(void);
+/* vortrace::warning_handler (include/mytypes.hpp:19-25; src/bindings.cpp:77-80).
+ * NULL restores the default (stderr "vortrace warning: <msg>"). */
+void vt_set_warning_callback(void (*cb)(const char *msg));
+/* Select the CUDA device used by handles created afterwards. */
+int vt_set_device(int device);
+
+/* ---- point cloud ------------------------------------------------------- */
+/* PointCloud() + PointCloud::loadPoints (src/pointcloud.cpp:12-191,
+ * src/bindings.cpp:29-69).  pos: npart x 3; fields: npart_fields x nfields;
+ * subbox: 6 values; vol: nvol values or NULL.  Filters to the padded box
+ * (non-periodic), builds orig_ids, checks valid_rgba and raises the
+ * reference's warnings through the warning callback. */
+int vt_cloud_create(const double *pos, uint64_t npart, const double *fields,
+                    uint64_t npart_fields, uint64_t nfields, const double *subbox,
+                    const double *vol, uint64_t nvol, int periodic, vt_cloud **out);
+/* PointCloud::buildTree (src/pointcloud.cpp:193-212): device build. */
+int vt_cloud_build_tree(vt_cloud *cloud);
+int vt_cloud_set_param(vt_cloud *cloud, int param, int64_t value);
+/* PointCloud getters (src/bindings.cpp:134-154). */
+int vt_cloud_get_info(const vt_cloud *cloud, vt_cloud_info *info);
+/* PointCloud::get_orig_ids: writes min(cap, npart) ids. */
+int vt_cloud_orig_ids(const vt_cloud *cloud, int64_t *out, uint64_t cap);
+void vt_cloud_destroy(vt_cloud *cloud);
+
+/* PointCloud::queryTree(q, k) (src/bindings.cpp:155-174): exact k-NN of nq
+ * query points (host buffers); ids are internal (filtered) indices, r2 the
+ * squared distances in the reference's summation order.  Missing entries
+ * (k > npart) get id -1 and r2 = DBL_MAX. */
+int vt_knn(const vt_cloud *cloud, const double *q, uint64_t nq, int k, int64_t *ids,
+           double *r2);
+
+/* ---- projections ------------------------------------------------------- */
+/* Projection(starts, ends) + makeProjection(cloud, mode) + returnProjection
+ * (src/projection.cpp:10-73, src/bindings.cpp:178-201).  Host buffers:
+ * starts/ends nrays x 3, out nrays x nout (nout = 3 for VOLUME, else
+ * nfields).  stats may be NULL. */
+int vt_project(vt_cloud *cloud, const double *starts, const double *ends, uint64_t nrays,
+               int mode, int kernel, double *out, vt_stats *stats);
+/* Same, on device buffers, enqueued on `stream` (a cudaStream_t, NULL for
+ * the handle's stream); returns after the launch has completed. */
+int vt_project_device(vt_cloud *cloud, const double *d_starts, const double *d_ends,
+                      uint64_t nrays, int mode, int kernel, double *d_out, void *stream,
+                      vt_stats *stats);
+
+/* makeDetailedProjection + returnSegments (src/projection.cpp:75-144,
+ * src/bindings.cpp:206-238).  Writes out (as vt_project) and the CSR
+ * offsets (nrays + 1 entries), and returns a library-owned segment list
+ * whose arrays are copied out with vt_segments_copy. */
+int vt_project_detailed(vt_cloud *cloud, const double *starts, const double *ends,
+                        uint64_t nrays, int mode, double *out, int64_t *offsets,
+                        vt_segments **segs);
+uint64_t vt_segments_count(const vt_segments *segs);
+/* cell_ids are internal (filtered) indices, as returnSegments gives them. */
+int vt_segments_copy(const vt_segments *segs, int64_t *cell_ids, double *s_enter,
+                     double *s_exit);
+void vt_segments_free(vt_segments *segs);
+
+/* Adjoint of vt_project with respect to the per-cell fields (no reference
+ * counterpart; the reference has no gradients).  grad_out: nrays x nout
+ * upstream gradient; out: the forward result (needed by VOLUME); grad_fields
+ * (npart x nfields, internal order) is accumulated into, not overwritten.
+ * SUM: grad[c,f] += grad_out[r,f] * ds over every segment of ray r in c.
+ * VOLUME: reverse-mode front-to-back compositing, transmittance recomputed
+ * by re-walking the ray. */
+int vt_project_adjoint(vt_cloud *cloud, const double *starts, const double *ends,
+                       uint64_t nrays, int mode, const double *out, const double *grad_out,
+                       double *grad_fields);
+int vt_project_adjoint_device(vt_cloud *cloud, const double *d_starts, const double *d_ends,
+                              uint64_t nrays, int mode, const double *d_out,
+                              const double *d_grad_out, double *d_grad_fields, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VORTRACE_B200_H */

@@ -1,0 +1,187 @@
+"""Regenerate the golden fixtures in tests/golden/ (run in a container that
+has the reference checkout and oracle/_ref built; not needed at test time).
+
+1. ``galaxy_interaction.npz``: the reference's own golden case
+   (tests/test_vortrace.py:12-32 in the reference): the snapshot
+   tests/test_data/galaxy_interaction.hdf5 (PartType0 Coordinates/Density as
+   float32, Parameters.BoxSize) and the expected 128x128 projection
+   tests/test_data/galaxy_interaction-proj.npy.  h5py is not installed, so
+   the uncompressed, contiguous datasets are read at their byte offsets; the
+   HDF5 signature, the sizes and the value ranges are checked, and the
+   projection produced from them by the reference module must match the
+   stored one at decimal=14 before anything is written.
+2. ``small_walks.npz``: segment lists (cell ids, s_enter, s_exit, offsets) and
+   integrate/max/min/volume outputs produced by the reference module
+   (oracle/_ref) on small seeded clouds: uniform, Plummer-clustered, a cubic
+   lattice with degenerate rays, and float32-quantised positions.
+
+Usage:  python tests/golden/make_golden.py [/path/to/reference]
+"""
+from __future__ import annotations
+
+import os
+import sys
+import warnings
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+
+SNAP_COORD_OFF, SNAP_DENS_OFF, SNAP_BOX_OFF = 19848, 1089052, 6800
+SNAP_N = 7217
+
+
+def read_snapshot(path):
+    raw = open(path, "rb").read()
+    if raw[:8] != b"\x89HDF\r\n\x1a\n":
+        raise ValueError("not an HDF5 file")
+    pos = np.frombuffer(raw, "<f4", SNAP_N * 3, SNAP_COORD_OFF).reshape(SNAP_N, 3).copy()
+    dens = np.frombuffer(raw, "<f4", SNAP_N, SNAP_DENS_OFF).copy()
+    box = float(np.frombuffer(raw, "<f8", 1, SNAP_BOX_OFF)[0])
+    if not (np.isfinite(pos).all() and np.isfinite(dens).all()):
+        raise ValueError("non-finite snapshot values")
+    if not (0 < box < 1e5 and pos.min() >= 0 and pos.max() <= box and dens.min() > 0):
+        raise ValueError("snapshot values out of range: wrong offsets?")
+    return pos, dens, box
+
+
+def galaxy(ref_root, mod):
+    td = os.path.join(ref_root, "tests", "test_data")
+    pos, dens, box = read_snapshot(os.path.join(td, "galaxy_interaction.hdf5"))
+    proj = np.load(os.path.join(td, "galaxy_interaction-proj.npy"))
+    # the reference test's call: ProjectionCloud(pos, dens, boundbox=[0,box]*3)
+    # -> grid_projection(extent=[box/2-37.5, box/2+37.5], 128, [0, box], None)
+    from vortrace_b200 import grid as G  # numpy-only module
+    length = 75.0
+    extent = [box / 2.0 - length / 2.0, box / 2.0 + length / 2.0]
+    gs, ge = G.generate_projection_grid(extent, 128, [0.0, box], None)
+    out, _, _ = O.reference_project(mod, pos, dens, [0.0, box] * 3, gs.reshape(-1, 3),
+                                    ge.reshape(-1, 3))
+    np.testing.assert_array_almost_equal(out.reshape(128, 128), proj, decimal=14)
+    np.savez_compressed(os.path.join(HERE, "galaxy_interaction.npz"), pos=pos, dens=dens,
+                        box_size=np.float64(box), proj=proj)
+    print("galaxy_interaction.npz written; max|ref-golden| =",
+          np.abs(out.reshape(128, 128) - proj).max())
+
+
+def lattice(n=5):
+    c = np.arange(n, dtype=np.float64)
+    xx, yy, zz = np.meshgrid(c, c, c, indexing="ij")
+    pos = np.column_stack([xx.ravel(), yy.ravel(), zz.ravel()])
+    return pos, [-0.5, n - 0.5] * 3
+
+
+LATTICE_RAYS = [
+    ([-0.1, -0.1, -0.1], [4.1, 4.1, 4.1]),     # body diagonal through vertices
+    ([0.5, 0.2, -0.1], [0.5, 0.2, 4.1]),       # along a face
+    ([0.5, 0.5, -0.1], [0.5, 0.5, 4.1]),       # along an edge
+    ([0.1, 0.1, 0.1], [0.9, 0.9, 0.9]),        # through one vertex
+    ([0.50001, 0.50001, -0.1], [0.50001, 0.50001, 4.1]),
+    ([2.0, 2.0, -0.5], [2.0, 2.0, 4.5]),
+    ([1.0, 2.0, -0.5], [1.0, 2.0, 4.5]),
+    ([3.0, 3.0, -0.5], [3.0, 3.0, 4.5]),
+    ([0.5, 0.5, 0.5], [0.6, 0.6, 0.6]),        # same cell
+    ([2.0, 2.0, -0.1], [2.0, 2.0, 4.1]),
+    ([4.1, 0.2, 3.3], [-0.2, 3.7, 0.4]),
+]
+
+
+def small_walks(mod):
+    rng = np.random.default_rng(20240601)
+    cases = {}
+
+    # uniform cloud, random rays, nf=2 (integrate/max/min)
+    n = 1500
+    pos = rng.uniform(0, 10, (n, 3))
+    f = np.column_stack([rng.lognormal(0, 1, n), rng.uniform(0, 1, n)])
+    st = rng.uniform(0, 10, (120, 3))
+    en = rng.uniform(0, 10, (120, 3))
+    cases["uniform"] = (pos, f, [0, 10] * 3, None, st, en, ["integrate", "max", "min"])
+
+    # Plummer-clustered cloud, z-grid rays
+    m = 2500
+    a = 0.5
+    u = rng.uniform(1e-6, 1, m)
+    r = a / np.sqrt(u ** (-2.0 / 3.0) - 1)
+    r = np.minimum(r, 4.0)
+    v = rng.normal(size=(m, 3))
+    v /= np.linalg.norm(v, axis=1)[:, None]
+    pos = 5.0 + r[:, None] * v
+    pos = np.vstack([pos, rng.uniform(0, 10, (250, 3))])
+    rho = (1 + np.sum((pos - 5) ** 2, axis=1) / a ** 2) ** -2.5
+    xs = np.linspace(4.0, 6.0, 10)
+    gx, gy = np.meshgrid(xs, xs, indexing="ij")
+    st = np.column_stack([gx.ravel(), gy.ravel(), np.zeros(gx.size)])
+    en = st.copy()
+    en[:, 2] = 10.0
+    cases["plummer"] = (pos, rho, [0, 10] * 3, None, st, en, ["integrate"])
+
+    # volume rendering on a random cloud (RGBA in range)
+    n = 1200
+    pos = rng.uniform(0, 10, (n, 3))
+    rgba = np.column_stack([rng.uniform(0, 1, (n, 3)), rng.uniform(0, 0.3, n)])
+    st = rng.uniform(0, 10, (100, 3))
+    en = rng.uniform(0, 10, (100, 3))
+    cases["volume"] = (pos, rgba, [0, 10] * 3, None, st, en, ["volume"])
+
+    # cubic lattice, degenerate rays (exact ties everywhere)
+    pos, bb = lattice(5)
+    st = np.array([c[0] for c in LATTICE_RAYS], float)
+    en = np.array([c[1] for c in LATTICE_RAYS], float)
+    cases["lattice"] = (pos, np.ones(len(pos)), bb, np.ones(len(pos)), st, en, ["integrate"])
+
+    # float32-quantised lattice (tests/test_degenerate.py:172-194 in the reference)
+    pos, bb = lattice(10)
+    off = np.array([500.0, 500.0, 500.1])
+    p32 = (pos + off).astype(np.float32)
+    p32 -= off.astype(np.float32)
+    pos = p32.astype(np.float64)
+    st = np.array([[-0.1, -0.1, -0.1], [0.3, -0.1, 0.2], [9.1, 0.0, 4.5]])
+    en = np.array([[9.1, 9.1, 9.1], [8.7, 9.2, 9.0], [0.0, 9.1, 4.5]])
+    cases["lattice_f32"] = (pos, np.ones(len(pos)), bb, np.ones(len(pos)), st, en, ["integrate"])
+
+    blob = {}
+    for name, (pos, f, bb, vol, st, en, modes) in cases.items():
+        blob[f"{name}/pos"] = pos
+        blob[f"{name}/fields"] = np.asarray(f, np.float64)
+        blob[f"{name}/bb"] = np.asarray(bb, np.float64)
+        if vol is not None:
+            blob[f"{name}/vol"] = np.asarray(vol, np.float64)
+        blob[f"{name}/starts"] = st
+        blob[f"{name}/ends"] = en
+        blob[f"{name}/modes"] = np.array(modes)
+        # the segment list does not depend on the reduction: store it once
+        for i, mode in enumerate(modes):
+            out, segs, oid = O.reference_project(mod, pos, f, bb, st, en, mode=mode, vol=vol,
+                                                 detailed=True)
+            cid, se, sx, off = segs
+            blob[f"{name}/{mode}/out"] = np.asarray(out).reshape(len(st), -1)
+            if i == 0:
+                blob[f"{name}/cell_ids"] = np.asarray(cid, np.int64)
+                blob[f"{name}/s_enter"] = np.asarray(se)
+                blob[f"{name}/s_exit"] = np.asarray(sx)
+                blob[f"{name}/offsets"] = np.asarray(off, np.int64)
+                blob[f"{name}/orig_ids"] = np.asarray(oid, np.int64)
+            else:
+                assert np.array_equal(blob[f"{name}/cell_ids"], cid)
+        print(name, "segments:", len(cid))
+    np.savez_compressed(os.path.join(HERE, "small_walks.npz"), **blob)
+    print("small_walks.npz written")
+
+
+def main():
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    mod = O.load_reference_module()
+    if mod is None:
+        raise SystemExit("oracle/_ref/Cvortrace not built: run oracle/build_ref.sh first")
+    warnings.simplefilter("ignore")
+    galaxy(ref_root, mod)
+    small_walks(mod)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,102 @@
+"""Build libvortrace_b200.so in-tree with nvcc (sm_100a only).
+
+    python -m vortrace_b200.build [--force] [--verbose-ptxas]
+
+Every .cu file under csrc/ is compiled for ``-gencode
+arch=compute_100a,code=sm_100a`` with ``--fmad=false`` (FP64 expressions must
+round like the reference's x86-64 build) and linked into
+``vortrace_b200/libvortrace_b200.so`` next to this file.
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libvortrace_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC",
+         "-Xcompiler", "-O3", "--expt-relaxed-constexpr", "-I" + INCLUDE]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found: cannot build libvortrace_b200")
+
+
+def host_compiler() -> list[str]:
+    # the system g++ (the environment's CXX may point at a toolchain without
+    # the libraries nvcc expects)
+    for cand in ("/usr/bin/g++", shutil.which("g++")):
+        if cand and os.path.exists(cand):
+            return ["-ccbin", cand]
+    return []
+
+
+def _sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+
+
+def _deps():
+    return _sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + sorted(
+        glob.glob(os.path.join(CSRC, "*.h"))) + [os.path.join(INCLUDE, "vortrace_b200.h"),
+                                                 os.path.abspath(__file__)]
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(d) <= t for d in _deps())
+
+
+def build(force: bool = False, ptxas_verbose: bool = False, jobs: int = 0) -> str:
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(BUILD, exist_ok=True)
+    cc = nvcc()
+    objs, procs = [], []
+    for src in _sources():
+        obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+        cmd = [cc, *ARCH, *FLAGS, *host_compiler(), "-c", src, "-o", obj]
+        if ptxas_verbose:
+            cmd += ["-Xptxas", "-v"]
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                                            text=True)))
+        objs.append(obj)
+    failed = False
+    for src, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            failed = True
+            sys.stderr.write(f"--- nvcc failed on {src}\n{out}\n")
+        elif out.strip():
+            sys.stderr.write(out)
+    if failed:
+        raise RuntimeError("libvortrace_b200 build failed")
+    tmp = LIB + ".tmp"
+    subprocess.run([cc, *ARCH, *host_compiler(), "-shared", *objs, "-o", tmp], check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose-ptxas", action="store_true")
+    a = ap.parse_args()
+    print(build(force=a.force, ptxas_verbose=a.verbose_ptxas))
+
+
+if __name__ == "__main__":
+    main()

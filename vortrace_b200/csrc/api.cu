@@ -1,0 +1,585 @@
+// api.cu -- the C ABI of libvortrace_b200 (include/vortrace_b200.h).
+//
+// Host side of the boundary the reference implements in src/bindings.cpp
+// (pybind11 module Cvortrace), src/pointcloud.cpp (loadPoints filtering,
+// padding, warnings, valid_rgba) and src/projection.cpp (driver).  Error and
+// warning texts are the reference's.
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <iostream>
+#include <limits>
+#include <memory>
+#include <new>
+
+#include "internal.h"
+
+#include "walkio.h"
+
+namespace vt {
+int run_knn(vt_cloud* cl, const double* d_q, int64_t nq, int k, int64_t* d_ids, double* d_r2,
+            cudaStream_t st);
+int scan_offsets(vt_cloud* cl, const int64_t* d_counts, int64_t* d_offsets, int64_t n,
+                 cudaStream_t st);
+}  // namespace vt
+
+namespace {
+thread_local std::string g_last_error;
+std::atomic<bool> g_verbose{false};
+std::mutex g_warn_mu;
+void (*g_warn_cb)(const char*) = nullptr;
+std::atomic<int> g_device{0};
+constexpr double kPi = 3.14159265358979323846;
+}  // namespace
+
+namespace vt {
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+void warn(const std::string& msg) {
+  std::lock_guard<std::mutex> lk(g_warn_mu);
+  if (g_warn_cb) g_warn_cb(msg.c_str());
+  else std::cerr << "vortrace warning: " << msg << std::endl;
+}
+bool verbose() { return g_verbose.load(); }
+}  // namespace vt
+
+using vt::set_error;
+
+#define VT_GUARD_BEGIN try {
+#define VT_GUARD_END                                                       \
+  }                                                                        \
+  catch (const std::bad_alloc&) {                                          \
+    return set_error(VT_ERR_NOMEM, "host allocation failed");             \
+  }                                                                        \
+  catch (const std::exception& e) {                                        \
+    return set_error(VT_ERR_RUNTIME, e.what());                           \
+  }
+
+static int check_projectable(const vt_cloud* cl, int mode) {
+  if (!cl) return set_error(VT_ERR_INVALID, "null cloud handle");
+  if (!cl->tree_built)
+    return set_error(VT_ERR_RUNTIME, "There is currently no valid tree for this point cloud");
+  if (mode < 0 || mode > 3) return set_error(VT_ERR_INVALID, "Unrecognized reduction mode");
+  if (mode == VT_REDUCE_VOLUME) {
+    if (cl->nfields != 4)
+      return set_error(VT_ERR_INVALID,
+                       "VolumeRender requires exactly 4 fields (R, G, B, alpha), got " +
+                           std::to_string(cl->nfields));
+    if (!cl->valid_rgba)
+      return set_error(VT_ERR_INVALID,
+                       "Volume rendering requires R, G, B values in [0, 1] and alpha >= 0");
+  }
+  if (cl->periodic)
+    return set_error(VT_ERR_RUNTIME,
+                     "periodic projections are not supported by libvortrace_b200 yet");
+  return VT_OK;
+}
+
+static int resolve_kernel(int kernel) {
+  if (kernel == VT_KERNEL_AUTO) return VT_KERNEL_BATCHED;
+  return kernel;
+}
+
+static cudaStream_t pick_stream(vt_cloud* cl, void* s) {
+  return s ? (cudaStream_t)s : cl->stream;
+}
+
+extern "C" {
+
+int vt_abi_version(void) { return VT_ABI_VERSION; }
+const char* vt_last_error(void) { return g_last_error.c_str(); }
+void vt_set_verbose(int v) { g_verbose.store(v != 0); }
+int vt_get_verbose(void) { return g_verbose.load() ? 1 : 0; }
+void vt_set_warning_callback(void (*cb)(const char*)) {
+  std::lock_guard<std::mutex> lk(g_warn_mu);
+  g_warn_cb = cb;
+}
+int vt_set_device(int device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+    return set_error(VT_ERR_CUDA, "no CUDA device available");
+  if (device < 0 || device >= n) return set_error(VT_ERR_INVALID, "invalid CUDA device index");
+  g_device.store(device);
+  return VT_OK;
+}
+
+int vt_cloud_create(const double* pos, uint64_t npart, const double* fields,
+                    uint64_t npart_fields, uint64_t nfields, const double* subbox,
+                    const double* vol, uint64_t nvol, int periodic, vt_cloud** out) {
+  VT_GUARD_BEGIN
+  if (!out) return set_error(VT_ERR_INVALID, "out must not be NULL");
+  *out = nullptr;
+  // src/bindings.cpp:53-56, src/pointcloud.cpp:18-22
+  if (npart != npart_fields)
+    return set_error(VT_ERR_INVALID, "Input sizes must match: pos has " + std::to_string(npart) +
+                                         " rows but fields has " + std::to_string(npart_fields));
+  if (!subbox) return set_error(VT_ERR_INVALID, "subbox must have 6 values");
+  if (npart > 0 && (!pos || !fields)) return set_error(VT_ERR_INVALID, "pos/fields must not be NULL");
+  if (nfields == 0) return set_error(VT_ERR_INVALID, "fields must have at least one column");
+  if (npart > (uint64_t)std::numeric_limits<int32_t>::max())
+    return set_error(VT_ERR_INVALID, "at most 2^31-1 points are supported");
+  if (nvol > 0 && !vol) return set_error(VT_ERR_INVALID, "vol must not be NULL when nvol > 0");
+
+  std::unique_ptr<vt_cloud> cl(new vt_cloud());
+  cl->device = g_device.load();
+  cl->nfields = nfields;
+  for (int i = 0; i < 6; ++i) cl->subbox[i] = subbox[i];
+  cl->periodic = periodic != 0;
+  const bool verbose = vt::verbose();
+
+  // src/pointcloud.cpp:38-53: small-cell warning
+  if (nvol > 0) {
+    double min_vol = std::numeric_limits<double>::max();
+    for (uint64_t i = 0; i < nvol; i++)
+      if (vol[i] > 0 && vol[i] < min_vol) min_vol = vol[i];
+    if (min_vol < std::numeric_limits<double>::max()) {
+      double min_radius = std::cbrt(3.0 * min_vol / (4.0 * kPi));
+      if (min_radius < 1e-6)
+        vt::warn(
+            "Some cells have radii smaller than 1e-6, which approaches the internal "
+            "ray-tracing tolerance (1e-9). Results may be unreliable for very small cells. "
+            "Consider rescaling your coordinate system.");
+    }
+  }
+  cl->pts.reserve(3 * npart);
+  cl->fields.reserve(nfields * npart);
+  if (!cl->periodic) {
+    // src/pointcloud.cpp:55-108: padding and filtering
+    const double dx = subbox[1] - subbox[0], dy = subbox[3] - subbox[2],
+                 dz = subbox[5] - subbox[4];
+    if (nvol > 0) {
+      double max_vol = 0.0;
+      for (uint64_t i = 0; i < nvol; i++)
+        if (vol[i] > max_vol) max_vol = vol[i];
+      cl->pad = 10.0 * std::cbrt(3.0 * max_vol / (4.0 * kPi));
+    } else {
+      cl->pad = 0.15 * std::max(dx, std::max(dy, dz));
+      vt::warn(
+          "No cell volumes provided; using 15% of longest box side as padding. Pass vol= for "
+          "adaptive padding.");
+    }
+    const double xmin = subbox[0] - cl->pad, xmax = subbox[1] + cl->pad;
+    const double ymin = subbox[2] - cl->pad, ymax = subbox[3] + cl->pad;
+    const double zmin = subbox[4] - cl->pad, zmax = subbox[5] + cl->pad;
+    if (verbose) std::cout << "Filtering and loading points...\n";
+    for (uint64_t i = 0; i < npart; i++) {
+      const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+      if (px >= xmin && px <= xmax && py >= ymin && py <= ymax && pz >= zmin && pz <= zmax) {
+        cl->pts.push_back(px);
+        cl->pts.push_back(py);
+        cl->pts.push_back(pz);
+        for (uint64_t f = 0; f < nfields; f++) cl->fields.push_back(fields[i * nfields + f]);
+        cl->orig_ids.push_back((int64_t)i);
+      }
+    }
+  } else {
+    // src/pointcloud.cpp:109-163: periodic, no filtering
+    cl->pad = 0.0;
+    if (verbose) std::cout << "Loading all points (periodic)...\n";
+    double pmin[3], pmax[3];
+    for (int d = 0; d < 3; ++d) {
+      pmin[d] = std::numeric_limits<double>::max();
+      pmax[d] = std::numeric_limits<double>::lowest();
+    }
+    for (uint64_t i = 0; i < npart; i++) {
+      for (int d = 0; d < 3; ++d) {
+        const double v = pos[3 * i + d];
+        cl->pts.push_back(v);
+        if (v < pmin[d]) pmin[d] = v;
+        if (v > pmax[d]) pmax[d] = v;
+      }
+      for (uint64_t f = 0; f < nfields; f++) cl->fields.push_back(fields[i * nfields + f]);
+      cl->orig_ids.push_back((int64_t)i);
+    }
+    if (pmin[0] < subbox[0] || pmax[0] > subbox[1] || pmin[1] < subbox[2] ||
+        pmax[1] > subbox[3] || pmin[2] < subbox[4] || pmax[2] > subbox[5])
+      return set_error(VT_ERR_INVALID,
+                       "Periodic mode: some particles lie outside the bounding box. All "
+                       "particles must be within the periodic domain.");
+    const double box[3] = {subbox[1] - subbox[0], subbox[3] - subbox[2], subbox[5] - subbox[4]};
+    for (int d = 0; d < 3; d++) {
+      if (pmax[d] - pmin[d] < 0.6 * box[d]) {
+        vt::warn(
+            "Periodic mode: particle extent is less than 60% of the bounding box in at least "
+            "one dimension. The bounding box may be too large for the particle distribution.");
+        break;
+      }
+    }
+  }
+  cl->npart = cl->orig_ids.size();
+  // src/pointcloud.cpp:167-179
+  cl->valid_rgba = false;
+  if (nfields == 4 && cl->npart > 0) {
+    cl->valid_rgba = true;
+    for (uint64_t i = 0; i < cl->npart && cl->valid_rgba; i++) {
+      for (int k = 0; k < 3; k++) {
+        const double v = cl->fields[i * 4 + k];
+        if (v < 0.0 || v > 1.0) {
+          cl->valid_rgba = false;
+          break;
+        }
+      }
+      if (cl->valid_rgba && cl->fields[i * 4 + 3] < 0.0) cl->valid_rgba = false;
+    }
+  }
+  if (verbose) {
+    if (!cl->periodic)
+      std::cout << "Filtered " << npart << " -> " << cl->npart << " particles\n";
+    else
+      std::cout << "Loaded " << cl->npart << " particles (periodic, no filtering)\n";
+    std::cout << "Padding: " << cl->pad << "\n";
+    std::cout << "Snapshot loaded." << std::endl;
+  }
+  if (cudaSetDevice(cl->device) != cudaSuccess)
+    return set_error(VT_ERR_CUDA, "cannot select CUDA device " + std::to_string(cl->device));
+  VT_CUDA(cudaStreamCreateWithFlags(&cl->stream, cudaStreamNonBlocking));
+  *out = cl.release();
+  return VT_OK;
+  VT_GUARD_END
+}
+
+void vt_cloud_destroy(vt_cloud* cl) {
+  if (!cl) return;
+  cudaSetDevice(cl->device);
+  if (cl->stream) {
+    cudaStreamSynchronize(cl->stream);
+    cudaStreamDestroy(cl->stream);
+  }
+  delete cl;
+}
+
+int vt_cloud_build_tree(vt_cloud* cl) {
+  VT_GUARD_BEGIN
+  if (!cl) return set_error(VT_ERR_INVALID, "null cloud handle");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  if (cl->npart == 0)
+    return set_error(VT_ERR_RUNTIME, "There are no points in the cloud; cannot build tree");
+  VT_CUDA(cudaSetDevice(cl->device));
+  if (vt::verbose()) std::cout << "Building tree...\n";
+  auto t0 = std::chrono::high_resolution_clock::now();
+  cl->tree_built = false;
+  int rc = vt::build_tree_device(cl);
+  if (rc) return rc;
+  auto t1 = std::chrono::high_resolution_clock::now();
+  cl->build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  cl->tree_built = true;
+  if (vt::verbose())
+    std::cout << "Tree build took " << (long long)cl->build_ms << " milliseconds." << std::endl;
+  return VT_OK;
+  VT_GUARD_END
+}
+
+int vt_cloud_set_param(vt_cloud* cl, int param, int64_t value) {
+  if (!cl) return set_error(VT_ERR_INVALID, "null cloud handle");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  switch (param) {
+    case VT_PARAM_MAX_ITERATIONS:
+      if (value < 1) return set_error(VT_ERR_INVALID, "max iterations must be >= 1");
+      cl->max_iter = value;
+      return VT_OK;
+    case VT_PARAM_STACK_CAP:
+      if (value < 2 || value > (1 << 22)) return set_error(VT_ERR_INVALID, "stack capacity out of range");
+      cl->stack_cap = (int)value;
+      return VT_OK;
+    case VT_PARAM_BLOCK_SIZE:
+      if (value != 128) return set_error(VT_ERR_INVALID, "block size must be 128");
+      cl->block_size = (int)value;
+      return VT_OK;
+    case VT_PARAM_SMEM_LEVELS:
+      if (value < 0 || value > 13) return set_error(VT_ERR_INVALID, "smem levels out of range [0, 13]");
+      cl->smem_levels = (int)value;
+      return VT_OK;
+    case VT_PARAM_BLOCKS_PER_SM:
+      if (value < 0 || value > 64) return set_error(VT_ERR_INVALID, "blocks per SM out of range");
+      cl->blocks_per_sm = (int)value;
+      return VT_OK;
+    case VT_PARAM_LEAF_SIZE:
+      if (value < 2 || value > 64) return set_error(VT_ERR_INVALID, "leaf size out of range [2, 64]");
+      cl->leaf_size = (int)value;
+      return VT_OK;
+    default:
+      return set_error(VT_ERR_INVALID, "unknown parameter " + std::to_string(param));
+  }
+}
+
+int vt_cloud_get_info(const vt_cloud* cl, vt_cloud_info* info) {
+  if (!cl || !info) return set_error(VT_ERR_INVALID, "null argument");
+  info->npart = cl->npart;
+  info->nfields = cl->nfields;
+  info->pad = cl->pad;
+  for (int i = 0; i < 6; ++i) info->subbox[i] = cl->subbox[i];
+  info->valid_rgba = cl->valid_rgba;
+  info->tree_built = cl->tree_built;
+  info->periodic = cl->periodic;
+  info->tree_depth = cl->tree_built ? cl->view.depth : 0;
+  info->tree_leaves = cl->tree_built ? (uint64_t)cl->view.nleaves : 0;
+  info->tree_build_ms = cl->build_ms;
+  info->device_bytes = cl->pts_d.bytes() + cl->pts32_d.bytes() + cl->nodes_d.bytes() +
+                       cl->nodes32_d.bytes() + cl->perm_d.bytes() + cl->fields_d.bytes();
+  return VT_OK;
+}
+
+int vt_cloud_orig_ids(const vt_cloud* cl, int64_t* out, uint64_t cap) {
+  if (!cl) return set_error(VT_ERR_INVALID, "null cloud handle");
+  const uint64_t n = cl->orig_ids.size() < cap ? cl->orig_ids.size() : cap;
+  if (n && !out) return set_error(VT_ERR_INVALID, "out must not be NULL");
+  if (n) memcpy(out, cl->orig_ids.data(), n * sizeof(int64_t));
+  return VT_OK;
+}
+
+int vt_knn(const vt_cloud* ccl, const double* q, uint64_t nq, int k, int64_t* ids, double* r2) {
+  VT_GUARD_BEGIN
+  vt_cloud* cl = const_cast<vt_cloud*>(ccl);
+  if (!cl) return set_error(VT_ERR_INVALID, "null cloud handle");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  if (!cl->tree_built)
+    return set_error(VT_ERR_RUNTIME, "There is currently no valid tree for this point cloud");
+  if (k < 1 || k > 128) return set_error(VT_ERR_INVALID, "k must be in [1, 128]");
+  if (nq == 0) return VT_OK;
+  VT_CUDA(cudaSetDevice(cl->device));
+  vt::DevBuf<double> dq, dr;
+  vt::DevBuf<int64_t> di;
+  int rc;
+  if ((rc = dq.alloc(3 * nq)) || (rc = dr.alloc(nq * k)) || (rc = di.alloc(nq * k))) return rc;
+  cudaStream_t st = cl->stream;
+  VT_CUDA(cudaMemcpyAsync(dq.p, q, 3 * nq * sizeof(double), cudaMemcpyHostToDevice, st));
+  if ((rc = vt::run_knn(cl, dq.p, (int64_t)nq, k, di.p, dr.p, st))) return rc;
+  VT_CUDA(cudaMemcpyAsync(ids, di.p, nq * k * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaMemcpyAsync(r2, dr.p, nq * k * sizeof(double), cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  return VT_OK;
+  VT_GUARD_END
+}
+
+static int project_device_locked(vt_cloud* cl, const double* d_starts, const double* d_ends,
+                                 uint64_t nrays, int mode, int kernel, double* d_out,
+                                 cudaStream_t st, vt_stats* stats, int out_kind,
+                                 int64_t* d_counts) {
+  vt::WalkIO io{};
+  io.starts = d_starts;
+  io.ends = d_ends;
+  io.nrays = (int64_t)nrays;
+  io.nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
+  io.out = d_out;
+  io.counts = d_counts;
+  return vt::run_walk(cl, io, out_kind, mode, resolve_kernel(kernel), st, stats);
+}
+
+int vt_project_device(vt_cloud* cl, const double* d_starts, const double* d_ends,
+                      uint64_t nrays, int mode, int kernel, double* d_out, void* stream,
+                      vt_stats* stats) {
+  VT_GUARD_BEGIN
+  int rc = check_projectable(cl, mode);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(cl->mu);
+  VT_CUDA(cudaSetDevice(cl->device));
+  if (stats) memset(stats, 0, sizeof(*stats));
+  if (nrays == 0) return VT_OK;
+  return project_device_locked(cl, d_starts, d_ends, nrays, mode, kernel, d_out,
+                               pick_stream(cl, stream), stats, vt::kOutImage, nullptr);
+  VT_GUARD_END
+}
+
+int vt_project(vt_cloud* cl, const double* starts, const double* ends, uint64_t nrays, int mode,
+               int kernel, double* out, vt_stats* stats) {
+  VT_GUARD_BEGIN
+  int rc = check_projectable(cl, mode);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(cl->mu);
+  VT_CUDA(cudaSetDevice(cl->device));
+  if (stats) memset(stats, 0, sizeof(*stats));
+  if (nrays == 0) return VT_OK;
+  const int nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
+  if ((rc = cl->ws_starts.reserve(3 * nrays)) || (rc = cl->ws_ends.reserve(3 * nrays)) ||
+      (rc = cl->ws_out.reserve(nrays * nout)))
+    return rc;
+  cudaStream_t st = cl->stream;
+  if (vt::verbose()) std::cout << "Making projection...\n";
+  auto t0 = std::chrono::high_resolution_clock::now();
+  VT_CUDA(cudaMemcpyAsync(cl->ws_starts.p, starts, 3 * nrays * sizeof(double),
+                          cudaMemcpyHostToDevice, st));
+  VT_CUDA(cudaMemcpyAsync(cl->ws_ends.p, ends, 3 * nrays * sizeof(double),
+                          cudaMemcpyHostToDevice, st));
+  rc = project_device_locked(cl, cl->ws_starts.p, cl->ws_ends.p, nrays, mode, kernel,
+                             cl->ws_out.p, st, stats, vt::kOutImage, nullptr);
+  if (rc) return rc;
+  VT_CUDA(cudaMemcpyAsync(out, cl->ws_out.p, nrays * nout * sizeof(double),
+                          cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  if (vt::verbose()) {
+    auto t1 = std::chrono::high_resolution_clock::now();
+    std::cout << "Projection generation took "
+              << (long long)std::chrono::duration<double, std::milli>(t1 - t0).count()
+              << " milliseconds." << std::endl;
+  }
+  return VT_OK;
+  VT_GUARD_END
+}
+
+int vt_project_detailed(vt_cloud* cl, const double* starts, const double* ends, uint64_t nrays,
+                        int mode, double* out, int64_t* offsets, vt_segments** segs) {
+  VT_GUARD_BEGIN
+  if (!segs || !offsets) return set_error(VT_ERR_INVALID, "segs/offsets must not be NULL");
+  *segs = nullptr;
+  int rc = check_projectable(cl, mode);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(cl->mu);
+  VT_CUDA(cudaSetDevice(cl->device));
+  std::unique_ptr<vt_segments> sg(new vt_segments());
+  sg->device = cl->device;
+  offsets[0] = 0;
+  if (nrays == 0) {
+    *segs = sg.release();
+    return VT_OK;
+  }
+  const int nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
+  if ((rc = cl->ws_starts.reserve(3 * nrays)) || (rc = cl->ws_ends.reserve(3 * nrays)) ||
+      (rc = cl->ws_out.reserve(nrays * nout)) || (rc = cl->ws_counts.reserve(2 * nrays + 1)))
+    return rc;
+  cudaStream_t st = cl->stream;
+  if (vt::verbose()) std::cout << "Making detailed projection...\n";
+  auto t0 = std::chrono::high_resolution_clock::now();
+  VT_CUDA(cudaMemcpyAsync(cl->ws_starts.p, starts, 3 * nrays * sizeof(double),
+                          cudaMemcpyHostToDevice, st));
+  VT_CUDA(cudaMemcpyAsync(cl->ws_ends.p, ends, 3 * nrays * sizeof(double),
+                          cudaMemcpyHostToDevice, st));
+  int64_t* d_counts = cl->ws_counts.p;
+  int64_t* d_off = cl->ws_counts.p + nrays;
+  // pass 1: reduction + segment counts
+  rc = project_device_locked(cl, cl->ws_starts.p, cl->ws_ends.p, nrays, mode,
+                             VT_KERNEL_PLAIN_FP64, cl->ws_out.p, st, nullptr, vt::kOutCount,
+                             d_counts);
+  if (rc) return rc;
+  if ((rc = vt::scan_offsets(cl, d_counts, d_off, (int64_t)nrays, st))) return rc;
+  VT_CUDA(cudaMemcpyAsync(offsets, d_off, (nrays + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                          st));
+  VT_CUDA(cudaMemcpyAsync(out, cl->ws_out.p, nrays * nout * sizeof(double),
+                          cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  const uint64_t total = (uint64_t)offsets[nrays];
+  if ((rc = sg->cell.alloc(total)) || (rc = sg->s_enter.alloc(total)) ||
+      (rc = sg->s_exit.alloc(total)))
+    return rc;
+  sg->count = total;
+  // pass 2: segments
+  vt::WalkIO io{};
+  io.starts = cl->ws_starts.p;
+  io.ends = cl->ws_ends.p;
+  io.nrays = (int64_t)nrays;
+  io.nout = nout;
+  io.offsets = d_off;
+  io.seg_cell = sg->cell.p;
+  io.seg_enter = sg->s_enter.p;
+  io.seg_exit = sg->s_exit.p;
+  rc = vt::run_walk(cl, io, vt::kOutFill, mode, VT_KERNEL_PLAIN_FP64, st, nullptr);
+  if (rc) return rc;
+  VT_CUDA(cudaStreamSynchronize(st));
+  if (vt::verbose()) {
+    auto t1 = std::chrono::high_resolution_clock::now();
+    std::cout << "Detailed projection generation took "
+              << (long long)std::chrono::duration<double, std::milli>(t1 - t0).count()
+              << " milliseconds." << std::endl;
+  }
+  *segs = sg.release();
+  return VT_OK;
+  VT_GUARD_END
+}
+
+uint64_t vt_segments_count(const vt_segments* s) { return s ? s->count : 0; }
+
+int vt_segments_copy(const vt_segments* s, int64_t* cell_ids, double* s_enter, double* s_exit) {
+  if (!s) return set_error(VT_ERR_INVALID, "null segments handle");
+  if (s->count == 0) return VT_OK;
+  VT_CUDA(cudaSetDevice(s->device));
+  if (cell_ids)
+    VT_CUDA(cudaMemcpy(cell_ids, s->cell.p, s->count * sizeof(int64_t), cudaMemcpyDeviceToHost));
+  if (s_enter)
+    VT_CUDA(cudaMemcpy(s_enter, s->s_enter.p, s->count * sizeof(double), cudaMemcpyDeviceToHost));
+  if (s_exit)
+    VT_CUDA(cudaMemcpy(s_exit, s->s_exit.p, s->count * sizeof(double), cudaMemcpyDeviceToHost));
+  return VT_OK;
+}
+
+void vt_segments_free(vt_segments* s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  delete s;
+}
+
+static int adjoint_locked(vt_cloud* cl, const double* d_starts, const double* d_ends,
+                          uint64_t nrays, int mode, const double* d_out,
+                          const double* d_gout, double* d_grad, cudaStream_t st) {
+  vt::WalkIO io{};
+  io.starts = d_starts;
+  io.ends = d_ends;
+  io.nrays = (int64_t)nrays;
+  io.nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
+  io.gout = d_gout;
+  io.fwd = d_out;
+  io.grad = d_grad;
+  return vt::run_walk(cl, io, vt::kOutAdj, mode, VT_KERNEL_BATCHED, st, nullptr);
+}
+
+int vt_project_adjoint_device(vt_cloud* cl, const double* d_starts, const double* d_ends,
+                              uint64_t nrays, int mode, const double* d_out,
+                              const double* d_grad_out, double* d_grad_fields, void* stream) {
+  VT_GUARD_BEGIN
+  int rc = check_projectable(cl, mode);
+  if (rc) return rc;
+  if (mode != VT_REDUCE_SUM && mode != VT_REDUCE_VOLUME)
+    return set_error(VT_ERR_INVALID, "adjoint is defined for 'integrate' and 'volume' only");
+  if (mode == VT_REDUCE_VOLUME && !d_out)
+    return set_error(VT_ERR_INVALID, "the volume adjoint needs the forward output");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  VT_CUDA(cudaSetDevice(cl->device));
+  if (nrays == 0) return VT_OK;
+  return adjoint_locked(cl, d_starts, d_ends, nrays, mode, d_out, d_grad_out, d_grad_fields,
+                        pick_stream(cl, stream));
+  VT_GUARD_END
+}
+
+int vt_project_adjoint(vt_cloud* cl, const double* starts, const double* ends, uint64_t nrays,
+                       int mode, const double* out, const double* grad_out,
+                       double* grad_fields) {
+  VT_GUARD_BEGIN
+  int rc = check_projectable(cl, mode);
+  if (rc) return rc;
+  if (mode != VT_REDUCE_SUM && mode != VT_REDUCE_VOLUME)
+    return set_error(VT_ERR_INVALID, "adjoint is defined for 'integrate' and 'volume' only");
+  if (mode == VT_REDUCE_VOLUME && !out)
+    return set_error(VT_ERR_INVALID, "the volume adjoint needs the forward output");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  VT_CUDA(cudaSetDevice(cl->device));
+  if (nrays == 0) return VT_OK;
+  const int nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
+  const uint64_t ng = cl->npart * cl->nfields;
+  if ((rc = cl->ws_starts.reserve(3 * nrays)) || (rc = cl->ws_ends.reserve(3 * nrays)) ||
+      (rc = cl->ws_out.reserve(nrays * nout)) || (rc = cl->ws_gout.reserve(nrays * nout)) ||
+      (rc = cl->ws_grad.reserve(ng)))
+    return rc;
+  cudaStream_t st = cl->stream;
+  VT_CUDA(cudaMemcpyAsync(cl->ws_starts.p, starts, 3 * nrays * sizeof(double),
+                          cudaMemcpyHostToDevice, st));
+  VT_CUDA(cudaMemcpyAsync(cl->ws_ends.p, ends, 3 * nrays * sizeof(double),
+                          cudaMemcpyHostToDevice, st));
+  if (out)
+    VT_CUDA(cudaMemcpyAsync(cl->ws_out.p, out, nrays * nout * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+  VT_CUDA(cudaMemcpyAsync(cl->ws_gout.p, grad_out, nrays * nout * sizeof(double),
+                          cudaMemcpyHostToDevice, st));
+  VT_CUDA(cudaMemcpyAsync(cl->ws_grad.p, grad_fields, ng * sizeof(double),
+                          cudaMemcpyHostToDevice, st));
+  rc = adjoint_locked(cl, cl->ws_starts.p, cl->ws_ends.p, nrays, mode, cl->ws_out.p,
+                      cl->ws_gout.p, cl->ws_grad.p, st);
+  if (rc) return rc;
+  VT_CUDA(cudaMemcpyAsync(grad_fields, cl->ws_grad.p, ng * sizeof(double),
+                          cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  return VT_OK;
+  VT_GUARD_END
+}
+
+}  // extern "C"

@@ -1,0 +1,513 @@
+// batched.cuh -- persistent walk kernel with bounded, guarded-FP32 k-NN.
+//
+// Same walk as walk_ray() (src/ray.cpp:187-430) restructured for SIMD
+// efficiency:
+//   * persistent grid (a multiple of the SM count); every lane owns one ray
+//     and takes a new one from a global atomic queue as soon as its ray is
+//     done (warp-aggregated atomicAdd), so long and short rays mix freely and
+//     many projections / arbitrary rays go through one launch;
+//   * one loop trip = one walk iteration per lane, so all lanes issue the
+//     same k-NN search code;
+//   * the split-point query is a *bounded* 3-NN: the two cells c and n whose
+//     bisector holds the split point are known, so the search starts with
+//     radius^2 R = max(d_c, d_n) + 4*TOL.  Every walk decision depends only
+//     on points with r^2 < R (proof in knn3_decision_valid), otherwise the
+//     query is re-resolved with an unbounded FP64 search;
+//   * guarded FP32: descent and distance tests run on FP32 copies (nodes32,
+//     pts32) with outward-rounded bounds; a point passes the FP32 test if
+//     f < thr64 + G where G bounds |f - d| (FP32 rounding of coordinates and
+//     arithmetic); every passing point is re-checked with its FP64 distance
+//     in the reference's operation order, so results are exact;
+//   * the top tree levels live in shared memory;
+//   * rare paths (parallel bisector fallback, Case 1a, 100-NN expansion, a
+//     pending-point stack deeper than the in-register one) hand the ray to
+//     k_slow with the number of segments already emitted.
+#pragma once
+
+namespace vt {
+
+constexpr int kBatchStack = 32;
+
+// ---- node fetch (shared memory for the top levels) ----------------------
+struct Fetch64 {
+  const double2* __restrict__ sm;
+  const double2* __restrict__ g;
+  int nsm;
+  __device__ __forceinline__ double2 operator()(int64_t i) const {
+    return i < nsm ? sm[i] : __ldg(&g[i]);
+  }
+};
+struct Fetch32 {
+  const float2* __restrict__ sm;
+  const float2* __restrict__ g;
+  int nsm;
+  __device__ __forceinline__ float2 operator()(int64_t i) const {
+    return i < nsm ? sm[i] : __ldg(&g[i]);
+  }
+};
+
+// Exact FP64 search with node fetch functor (same algorithm as knn_exact64).
+template <class List, class F>
+__device__ __forceinline__ void knn64_fetch(const DevCloud& c, const F& fetch, double qx,
+                                            double qy, double qz, double bound, List& res,
+                                            unsigned& nvisit) {
+  const double q[3] = {qx, qy, qz};
+  double off[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (q[d] < c.bblo[d]) off[d] = dmul(dsub(q[d], c.bblo[d]), dsub(q[d], c.bblo[d]));
+    if (q[d] > c.bbhi[d]) off[d] = dmul(dsub(q[d], c.bbhi[d]), dsub(q[d], c.bbhi[d]));
+  }
+  double thr = fmin(bound, res.worst());
+  const int64_t ninternal = c.nleaves - 1;
+  int node = 0;
+  int sp = 0;
+  int s_node[kMaxDepth + 2];
+  float s_mind[kMaxDepth + 2];
+  float s_off[kMaxDepth + 2][3];
+  unsigned visits = 0;
+  for (;;) {
+    ++visits;
+    if (node < ninternal) {
+      const double2 nd = fetch(node);
+      const int dim = node_dim(nd.x);
+      const double val = q[dim];
+      const double diff1 = dsub(val, nd.x);
+      const double diff2 = dsub(val, nd.y);
+      const int first = 2 * node + 1;
+      int best, other;
+      double cut;
+      if (dadd(diff1, diff2) < 0) {
+        best = first;
+        other = first + 1;
+        cut = dmul(diff2, diff2);
+      } else {
+        best = first + 1;
+        other = first;
+        cut = dmul(diff1, diff1);
+      }
+      const double o0 = dim == 0 ? cut : off[0];
+      const double o1 = dim == 1 ? cut : off[1];
+      const double o2 = dim == 2 ? cut : off[2];
+      const double nm = dmul(dadd(dadd(o0, o1), o2), 0.9999999999999991);
+      if (nm < thr) {
+        s_node[sp] = other;
+        s_mind[sp] = __double2float_rd(nm);
+        s_off[sp][0] = __double2float_rd(o0);
+        s_off[sp][1] = __double2float_rd(o1);
+        s_off[sp][2] = __double2float_rd(o2);
+        ++sp;
+      }
+      node = best;
+      continue;
+    }
+    {
+      int64_t a, b;
+      leaf_range(c, node - ninternal, a, b);
+      for (int64_t p = a; p < b; ++p) {
+        const double d = metric(qx, qy, qz, ldg_pt(&c.pts[p]));
+        if (d < thr) {
+          res.insert(d, (int)p);
+          thr = fmin(bound, res.worst());
+        }
+      }
+    }
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      if ((double)s_mind[sp] < thr) {
+        node = s_node[sp];
+        off[0] = s_off[sp][0];
+        off[1] = s_off[sp][1];
+        off[2] = s_off[sp][2];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  nvisit += visits;
+}
+
+// Guarded FP32 bounded search.  Accepts points with FP64 distance d < R,
+// keeps the 3 nearest (stable insertion).  G bounds |f - d| for every point
+// with d < R, where f is the FP32 distance from pts32.  dc/dn: the known
+// FP64 distances of the cells cid/nid (no reload).
+template <class F>
+__device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, double qx,
+                                             double qy, double qz, int cid, int nid, double dc,
+                                             double dn, double R, double G, KnnList<3>& res,
+                                             unsigned& nvisit, unsigned& nverify) {
+  const float q32[3] = {__double2float_rn(dsub(qx, c.origin[0])),
+                        __double2float_rn(dsub(qy, c.origin[1])),
+                        __double2float_rn(dsub(qz, c.origin[2]))};
+  res.clear();
+  double thr64 = R;
+  float thr32 = __double2float_ru(dadd(thr64, G));
+  float off[3] = {0.f, 0.f, 0.f};
+  const int64_t ninternal = c.nleaves - 1;
+  int node = 0;
+  int sp = 0;
+  int s_node[kMaxDepth + 2];
+  float s_off[kMaxDepth + 2][3];
+  float s_mind[kMaxDepth + 2];
+  unsigned visits = 0, ver = 0;
+  for (;;) {
+    ++visits;
+    if (node < ninternal) {
+      const float2 nd = fetch(node);
+      const int dim = node_dim32(nd.x);
+      const float val = q32[dim];
+      const int first = 2 * node + 1;
+      int best, other;
+      float o;
+      if (__fadd_rn(__fsub_rn(val, nd.x), __fsub_rn(val, nd.y)) < 0.f) {
+        best = first;
+        other = first + 1;
+        o = nd.y > val ? __fsub_rn(nd.y, val) : 0.f;  // right child: p >= hi32
+      } else {
+        best = first + 1;
+        other = first;
+        o = val > nd.x ? __fsub_rn(val, nd.x) : 0.f;  // left child: p <= lo32
+      }
+      const float t = __fmul_rn(o, o);
+      const float o0 = dim == 0 ? t : off[0];
+      const float o1 = dim == 1 ? t : off[1];
+      const float o2 = dim == 2 ? t : off[2];
+      const float nm = __fadd_rn(__fadd_rn(o0, o1), o2);
+      if (nm < thr32) {
+        s_node[sp] = other;
+        s_mind[sp] = nm;
+        s_off[sp][0] = o0;
+        s_off[sp][1] = o1;
+        s_off[sp][2] = o2;
+        ++sp;
+      }
+      node = best;
+      continue;
+    }
+    {
+      int64_t a, b;
+      leaf_range(c, node - ninternal, a, b);
+      for (int64_t p = a; p < b; ++p) {
+        const float4 P = __ldg(&c.pts32[p]);
+        const float d0 = __fsub_rn(q32[0], P.x), d1 = __fsub_rn(q32[1], P.y),
+                    d2 = __fsub_rn(q32[2], P.z);
+        const float f =
+            __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
+        if (f < thr32) {
+          const int pi = (int)p;
+          double d;
+          if (pi == cid) d = dc;
+          else if (pi == nid) d = dn;
+          else {
+            d = metric(qx, qy, qz, ldg_pt(&c.pts[p]));
+            ++ver;
+          }
+          if (d < thr64) {
+            res.insert(d, pi);
+            thr64 = fmin(R, res.worst());
+            thr32 = __double2float_ru(dadd(thr64, G));
+          }
+        }
+      }
+    }
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      if (s_mind[sp] < thr32) {
+        node = s_node[sp];
+        off[0] = s_off[sp][0];
+        off[1] = s_off[sp][1];
+        off[2] = s_off[sp][2];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  nvisit += visits;
+  nverify += ver;
+}
+
+// A bounded result B (all points with d < R, at most 3, exact order) gives
+// the same walk decisions as the unbounded 3-NN T when:
+//   * |B| == 3 (then B == T), or
+//   * |B| >= 1 and fl(R - r2[0]) >= TOL and fl(r2[0] + TOL) < R: every
+//     missing entry of T has r2 >= R, so by monotone rounding the loop
+//     "r2[i] - r2[0] >= TOL" breaks at the same i and "r2[0] + TOL < r2[1]"
+//     has the same truth value.
+__device__ __forceinline__ bool knn3_decision_valid(const KnnList<3>& r, double R) {
+  const int cnt = r.count();
+  if (cnt == 3) return true;
+  if (cnt == 0) return false;
+  return dsub(R, r.r2[0]) >= kTol && dadd(r.r2[0], kTol) < R;
+}
+
+// Bound on |f - d| for points with d < R (see knn3_guarded).
+__device__ __forceinline__ double guard_band(double R, double e) {
+  const double u = 5.9604644775390625e-08;  // 2^-24
+  const double sr = sqrt(R);
+  const double cross = 3.5 * e * sr + 3.0 * e * e;
+  return 1.02 * (6.0 * u * (R + cross) + cross + 1e-15 * R);
+}
+
+// --------------------------------------------------------------- kernel
+template <int MODE, int NF, int OUT, bool G32>
+__global__ void __launch_bounds__(128) k_batched(DevCloud c, WalkIO io, int nsm) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // stage the top tree levels
+  if (G32) {
+    float2* s = reinterpret_cast<float2*>(smem_raw);
+    for (int i = threadIdx.x; i < nsm; i += blockDim.x) s[i] = c.nodes32[i];
+  } else {
+    double2* s = reinterpret_cast<double2*>(smem_raw);
+    for (int i = threadIdx.x; i < nsm; i += blockDim.x) s[i] = c.nodes[i];
+  }
+  __syncthreads();
+  const Fetch64 f64{reinterpret_cast<const double2*>(smem_raw), c.nodes, G32 ? 0 : nsm};
+  const Fetch32 f32{reinterpret_cast<const float2*>(smem_raw), c.nodes32, G32 ? nsm : 0};
+
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const double cerr = (double)c.coord_err;
+
+  // per-lane ray state
+  int64_t ray = -1;
+  int phase = 0;  // 0 idle, 1 start query, 2 end query, 3 walking
+  bool exhausted = false;
+  RayGeom g;
+  int c0 = -1, cur = -1, open_cell = -1, nxt = -1;
+  double cur_s = 0.0, entry_s = 0.0, nxt_s = 0.0, s_split = 0.0;
+  int64_t iter = 0;
+  LocalStack<kBatchStack> st;
+  st.clear();
+  double q_err = 0.0;
+  // sinks
+  Reducer<MODE, NF> red;
+  FillSink fill;
+  AdjSink<MODE, NF> adj;
+  // lane counters
+  unsigned n_rays = 0, n_cross = 0, n_q = 0, n_res = 0, n_visit = 0, n_ver = 0, max_sp = 0;
+
+  for (;;) {
+    // ---- refill idle lanes from the work queue
+    const bool want = (phase == 0) && !exhausted;
+    const unsigned need = __ballot_sync(FULL, want);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(&io.stats->next_ray, (unsigned long long)__popc(need));
+      base = __shfl_sync(FULL, base, leader);
+      if (want) {
+        const int64_t r = (int64_t)base + __popc(need & ((1u << lane) - 1));
+        if (r < io.nrays) {
+          ray = r;
+          ray_init(g, io.starts + 3 * r, io.ends + 3 * r);
+          if (!ray_finite(g)) {
+            report(io, r, kErrNonFinite);
+          } else {
+            phase = 1;
+            ++n_rays;
+            if (OUT == kOutImage || OUT == kOutCount) red.init(&c, io.out + r * io.nout);
+            else if (OUT == kOutFill) fill.init(&c, io, r);
+            else adj.init(&c, io, r, 0u);
+            double m = 0.0;
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+              m = fmax(m, fmax(fabs(g.s[j] - c.origin[j]), fabs(g.e[j] - c.origin[j])));
+            q_err = m * 6.0e-8 + cerr;
+          }
+        } else {
+          exhausted = true;
+        }
+      }
+    }
+    if (__all_sync(FULL, phase == 0 && exhausted)) break;
+
+    unsigned nseg_now = 0;
+    auto nseg_of = [&]() -> unsigned {
+      if (OUT == kOutImage || OUT == kOutCount) return red.nseg;
+      if (OUT == kOutFill) return fill.nseg;
+      return adj.nseg;
+    };
+    auto emit = [&](int cell, double a, double b) {
+      if (OUT == kOutImage || OUT == kOutCount) red.seg(cell, a, b);
+      else if (OUT == kOutFill) fill.seg(cell, a, b);
+      else adj.seg(cell, a, b);
+    };
+    auto finish_ok = [&]() {
+      if (OUT == kOutImage || OUT == kOutCount) {
+        red.write(io.out + ray * io.nout);
+        if (OUT == kOutCount) io.counts[ray] = red.nseg;
+      }
+      n_cross += nseg_of();
+      max_sp = max(max_sp, (unsigned)st.maxsp);
+      phase = 0;
+    };
+    auto fail = [&](int rc) {
+      if (rc == kNeedSlow) hand_over(io, ray, nseg_of());
+      else report(io, ray, rc);
+      max_sp = max(max_sp, (unsigned)st.maxsp);
+      phase = 0;
+    };
+    (void)nseg_now;
+
+    // ---- prepare this lane's query
+    int qkind = 0;  // 0 none, 1 nearest neighbour (FP64), 2 bounded 3-NN
+    double qx = 0, qy = 0, qz = 0, dc = 0, dn = 0, R = 0;
+    if (phase == 1) {
+      qx = g.s[0]; qy = g.s[1]; qz = g.s[2];
+      qkind = 1;
+    } else if (phase == 2) {
+      qx = g.e[0]; qy = g.e[1]; qz = g.e[2];
+      qkind = 1;
+    } else if (phase == 3) {
+      for (;;) {
+        if (++iter > io.max_iter) {
+          fail(kErrMaxIter);
+          break;
+        }
+        nxt = st.top_id();
+        nxt_s = st.top_s();
+        if (dsub(nxt_s, cur_s) < 1e-14) {  // zero-width skip
+          st.pop();
+          cur = nxt;
+          cur_s = nxt_s;
+          open_cell = cur;
+          if (st.empty()) {
+            emit(open_cell, entry_s, cur_s);
+            finish_ok();
+            break;
+          }
+          continue;
+        }
+        const double4 pc = ldg_pt(&c.pts[cur]);
+        const double4 pn = ldg_pt(&c.pts[nxt]);
+        double s = split_analytic(g, pc, pn);
+        if (!(s < DBL_MAX * 0.5 && s >= cur_s - kTol && s <= nxt_s + kTol)) {
+          fail(kNeedSlow);  // parallel-bisector bisection search
+          break;
+        }
+        {
+          const double lo = dadd(cur_s, 1e-15), hi = dsub(nxt_s, 1e-15);
+          s = (s < lo) ? lo : (hi < s) ? hi : s;
+        }
+        s_split = s;
+        ray_point(g, s, qx, qy, qz);
+        dc = metric(qx, qy, qz, pc);
+        dn = metric(qx, qy, qz, pn);
+        R = dadd(fmax(dc, dn), 4.0 * kTol);
+        qkind = 2;
+        break;
+      }
+    }
+
+    // ---- search (lanes of one kind run the same code)
+    KnnList<3> r;
+    if (qkind == 1) {
+      r.clear();
+      ++n_q;
+      knn64_fetch(c, f64, qx, qy, qz, pinf(), r, n_visit);
+    } else if (qkind == 2) {
+      ++n_q;
+      if (G32) {
+        const double G = guard_band(R, q_err);
+        knn3_guarded(c, f32, qx, qy, qz, cur, nxt, dc, dn, R, G, r, n_visit, n_ver);
+      } else {
+        r.clear();
+        knn64_fetch(c, f64, qx, qy, qz, R, r, n_visit);
+      }
+      if (!knn3_decision_valid(r, R)) {
+        ++n_res;
+        r.clear();
+        knn64_fetch(c, f64, qx, qy, qz, pinf(), r, n_visit);
+      }
+    }
+
+    // ---- apply
+    if (qkind == 1 && phase == 1) {
+      c0 = r.id[0];
+      phase = 2;
+    } else if (qkind == 1 && phase == 2) {
+      const int c1 = r.id[0];
+      if (c0 == c1) {
+        emit(c0, 0.0, g.len);
+        finish_ok();
+      } else {
+        st.clear();
+        st.push(c1, g.len);
+        cur = c0;
+        cur_s = 0.0;
+        open_cell = c0;
+        entry_s = 0.0;
+        iter = 0;
+        phase = 3;
+      }
+    } else if (qkind == 2) {
+      bool has_c = false, has_n = false, three_eq = true;
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        if (dsub(r.r2[i], r.r2[0]) >= kTol) {
+          three_eq = false;
+          break;
+        }
+        if (r.id[i] == cur) has_c = true;
+        if (r.id[i] == nxt) has_n = true;
+      }
+      if (three_eq && !has_c && !has_n) {
+        fail(kNeedSlow);  // 100-NN expansion
+      } else if (has_c || has_n) {
+        emit(open_cell, entry_s, s_split);
+        open_cell = nxt;
+        entry_s = s_split;
+        st.pop();
+        cur = nxt;
+        cur_s = nxt_s;
+        if (st.empty()) {
+          emit(open_cell, entry_s, cur_s);
+          finish_ok();
+        }
+      } else if (dadd(r.r2[0], kTol) < r.r2[1]) {
+        if (st.room() < 1) fail(kNeedSlow);
+        else st.push(r.id[0], s_split);
+      } else {
+        fail(kNeedSlow);  // Case 1a
+      }
+    }
+  }
+  warp_add(&io.stats->rays, n_rays);
+  warp_add(&io.stats->crossings, n_cross);
+  warp_add(&io.stats->queries, n_q);
+  warp_add(&io.stats->fp64_resolves, n_res);
+  warp_max(&io.stats->max_stack, max_sp);
+}
+
+template <int MODE, int NF, int OUT>
+int launch_batched(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) {
+  const bool g32 = kernel != VT_KERNEL_BATCHED_FP64;
+  const int64_t ninternal = cl->view.nleaves - 1;
+  int64_t want = (1LL << cl->smem_levels) - 1;
+  int nsm = (int)(want < ninternal ? want : ninternal);
+  if (nsm < 0) nsm = 0;
+  const size_t smem = (size_t)nsm * (g32 ? sizeof(float2) : sizeof(double2));
+  const int B = 128;
+  int dev = 0, nsms = 0;
+  VT_CUDA(cudaGetDevice(&dev));
+  VT_CUDA(cudaDeviceGetAttribute(&nsms, cudaDevAttrMultiProcessorCount, dev));
+  auto kfun = g32 ? k_batched<MODE, NF, OUT, true> : k_batched<MODE, NF, OUT, false>;
+  if (smem > 48 * 1024)
+    VT_CUDA(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = cl->blocks_per_sm;
+  if (per_sm <= 0) {
+    VT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, B, smem));
+    if (per_sm < 1) per_sm = 1;
+  }
+  int64_t blocks = (int64_t)nsms * per_sm;
+  const int64_t need = (io.nrays + B - 1) / B;
+  if (blocks > need) blocks = need > 0 ? need : 1;
+  kfun<<<(unsigned)blocks, B, smem, st>>>(cl->view, io, nsm);
+  return VT_OK;
+}
+
+}  // namespace vt

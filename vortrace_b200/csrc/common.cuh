@@ -1,0 +1,120 @@
+// common.cuh -- device-side types shared by the tree build, the k-NN
+// searches and the walk kernels of libvortrace_b200.
+//
+// HBM layout of a built cloud (all arrays in *tree order*: the order of the
+// implicit tree's leaves, see tree_build.cu):
+//   pts     double4[n]   (x, y, z, unused)            32 B / point, one sector
+//   pts32   float4[n]    (p - origin) in FP32, w = 0  16 B / point
+//   nodes   double2[L-1] {divlow | split dim in the two low mantissa bits
+//                         (rounded up), divhigh}      16 B / internal node
+//   nodes32 float2[L-1]  {divlow rounded up | dim, divhigh rounded down},
+//                         relative to origin           8 B / internal node
+//   perm    int32[n]     tree index -> internal (filtered) point id
+//   fields  double[n*nf] per-point fields, tree order
+// The tree is implicit: internal node i has children 2i+1 and 2i+2, the
+// L = 2^depth leaves follow the L-1 internal nodes, and leaf j holds the
+// points [(j*n)>>depth, ((j+1)*n)>>depth).
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vt {
+
+// Constants of the reference walk (src/ray.cpp:8-12, :321)
+constexpr double kTol = 1e-9;
+constexpr double kParallelTol = 1e-12;
+constexpr double kPerturbEps = 2 * kTol;
+constexpr int kMaxPerturbCycles = 1000;
+constexpr int kExpandK = 100;
+constexpr int kMaxDepth = 30;  // internal tree levels supported
+
+// status codes (include/vortrace_b200.h)
+constexpr int kErrMaxIter = 10;
+constexpr int kErrSplitBounds = 11;
+constexpr int kErrBinSearch = 12;
+constexpr int kErrPerturb = 13;
+constexpr int kErrKnnExpand = 14;
+constexpr int kErrStack = 15;
+// internal: the ray must be finished by the degenerate-geometry kernel
+constexpr int kNeedSlow = 99;
+
+enum Mode { kSum = 0, kMax = 1, kMin = 2, kVolume = 3 };
+
+struct DevCloud {
+  const double4* __restrict__ pts;
+  const float4* __restrict__ pts32;
+  const double2* __restrict__ nodes;
+  const float2* __restrict__ nodes32;
+  const int32_t* __restrict__ perm;
+  const double* __restrict__ fields;
+  int64_t n;
+  int64_t nleaves;  // 2^depth
+  int nf;
+  int depth;
+  double bblo[3], bbhi[3];  // tight box of all points (nanoflann root_bbox)
+  double origin[3];         // frame of pts32 / nodes32
+  float coord_err;          // bound on |pts32 - (p - origin)| per component
+};
+
+// ---- FP64 arithmetic with the reference's rounding (no FMA contraction) --
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// nanoflann L2_Simple_Adaptor::evalMetric (include/nanoflann.hpp:432-439):
+// ((0 + d0*d0) + d1*d1) + d2*d2, d = q - p.  0 + x == x exactly.
+__device__ __forceinline__ double metric(double qx, double qy, double qz, double4 p) {
+  double d0 = dsub(qx, p.x), d1 = dsub(qy, p.y), d2 = dsub(qz, p.z);
+  return dadd(dadd(dmul(d0, d0), dmul(d1, d1)), dmul(d2, d2));
+}
+
+// read-only 32-byte point load (two 16-byte halves of one sector)
+__device__ __forceinline__ double4 ldg_pt(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  const double2 a = __ldg(q), b = __ldg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ int node_dim(double lo) {
+  return (int)(__double_as_longlong(lo) & 3);
+}
+__device__ __forceinline__ int node_dim32(float lo) { return (int)(__float_as_uint(lo) & 3u); }
+
+__device__ __forceinline__ void leaf_range(const DevCloud& c, int64_t leaf, int64_t& a,
+                                           int64_t& b) {
+  a = (leaf * c.n) >> c.depth;
+  b = ((leaf + 1) * c.n) >> c.depth;
+}
+
+// Per-launch counters (atomically accumulated, warp-aggregated).
+struct DevStats {
+  unsigned long long rays;
+  unsigned long long crossings;
+  unsigned long long queries;
+  unsigned long long fp64_resolves;
+  unsigned long long slow_rays;
+  unsigned long long max_stack;
+  unsigned long long first_error;  // (ray << 8) | code, ~0 when none
+  unsigned long long slow_count;   // rays queued for the degenerate kernel
+  unsigned long long next_ray;     // work-queue head of the batched kernel
+  unsigned long long next_slow;    // work-queue head of the degenerate kernel
+  unsigned long long pad[6];
+};
+
+// Sum a small per-lane value over the active lanes, one atomic per warp.
+__device__ __forceinline__ void warp_add(unsigned long long* p, unsigned v) {
+  unsigned mask = __activemask();
+  unsigned s = __reduce_add_sync(mask, v);
+  if ((int)(threadIdx.x & 31) == __ffs(mask) - 1 && s) atomicAdd(p, (unsigned long long)s);
+}
+
+__device__ __forceinline__ void warp_max(unsigned long long* p, unsigned v) {
+  unsigned mask = __activemask();
+  unsigned s = __reduce_max_sync(mask, v);
+  if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) atomicMax(p, (unsigned long long)s);
+}
+
+}  // namespace vt

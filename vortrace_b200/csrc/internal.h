@@ -1,0 +1,127 @@
+// internal.h -- host-side internals of libvortrace_b200 (not installed).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/vortrace_b200.h"
+#include "common.cuh"
+
+namespace vt {
+
+// Record the message of a failing call for vt_last_error() on this thread;
+// returns `code` so call sites can `return set_error(...)`.
+int set_error(int code, const std::string& msg);
+void warn(const std::string& msg);
+bool verbose();
+
+#define VT_CUDA(call)                                                                      \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return ::vt::set_error(VT_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e_) + \
+                                              " at " + __FILE__ + ":" + std::to_string(__LINE__)); \
+  } while (0)
+
+// Owning device buffer of T (cudaMalloc/cudaFree).
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      reset();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  int alloc(size_t count) {
+    reset();
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return set_error(VT_ERR_NOMEM, std::string("device allocation of ") +
+                                         std::to_string(count * sizeof(T)) +
+                                         " bytes failed: " + cudaGetErrorString(e));
+    }
+    n = count;
+    return VT_OK;
+  }
+  // grow-only (contents not preserved)
+  int reserve(size_t count) { return count <= n ? VT_OK : alloc(count); }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+}  // namespace vt
+
+struct vt_segments {
+  vt::DevBuf<int64_t> cell;
+  vt::DevBuf<double> s_enter, s_exit;
+  uint64_t count = 0;
+  int device = 0;
+};
+
+struct vt_cloud {
+  std::mutex mu;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // loadPoints state (src/pointcloud.cpp:12-191)
+  uint64_t npart = 0, nfields = 1;
+  double pad = 0.0;
+  double subbox[6] = {0, 0, 0, 0, 0, 0};
+  bool periodic = false, valid_rgba = false, tree_built = false;
+  std::vector<double> pts;     // filtered, internal order, n x 3
+  std::vector<double> fields;  // filtered, n x nfields
+  std::vector<int64_t> orig_ids;
+  // parameters
+  int64_t max_iter = 100000;
+  int stack_cap = 4096;
+  int leaf_size = 8;
+  int block_size = 128;
+  int smem_levels = 9;
+  int blocks_per_sm = 0;
+  // device tree (tree order)
+  vt::DevBuf<double4> pts_d;
+  vt::DevBuf<float4> pts32_d;
+  vt::DevBuf<double2> nodes_d;
+  vt::DevBuf<float2> nodes32_d;
+  vt::DevBuf<int32_t> perm_d;
+  vt::DevBuf<double> fields_d;
+  vt::DevCloud view{};
+  double build_ms = 0.0;
+  // per-call workspace (grow-only)
+  vt::DevBuf<double> ws_starts, ws_ends, ws_out, ws_gout, ws_grad;
+  vt::DevBuf<int64_t> ws_counts;
+  vt::DevBuf<unsigned long long> ws_slow;
+  vt::DevBuf<int> ws_stack_id;
+  vt::DevBuf<double> ws_stack_s;
+  vt::DevBuf<vt::DevStats> ws_stats;
+  vt::DevBuf<uint8_t> ws_tmp;
+};
+
+namespace vt {
+int build_tree_device(vt_cloud* cl);
+}

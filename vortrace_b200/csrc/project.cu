@@ -1,0 +1,504 @@
+// project.cu -- walk kernels, fused reductions, segment output, adjoint.
+//
+// Replaces Projection::makeProjection / makeDetailedProjection
+// (src/projection.cpp:26-144), Ray::integrate (src/ray.cpp:432-442) and the
+// reductions (src/reduction.cpp:8-96).
+//
+// Kernels
+//   k_plain   one ray per thread, exact FP64 k-NN searched from the root for
+//             every query (the straightforward port; the baseline kernel);
+//   k_batched persistent kernel (batched.cuh): atomic work queue, bounded
+//             guarded-FP32 k-NN, top tree levels in shared memory;
+//   k_slow    finishes the rays the two above hand over (degenerate
+//             geometry: parallel bisectors, Case 1a, 100-NN expansion, or a
+//             pending-point stack deeper than the in-register one), with
+//             every rare path of the reference and a global-memory stack;
+//   k_diag    re-walks the first failing ray alone to recover the numbers of
+//             the reference's error message.
+// Output kinds: image (reduction per ray), count (image + segments per
+// ray), fill (CSR segments), adjoint (scatter-add of field gradients).
+#include <cub/cub.cuh>
+
+#include <chrono>
+#include <cstdio>
+
+#include "internal.h"
+#include "walk.cuh"
+#include "walkio.h"
+
+namespace vt {
+
+constexpr int kPlainStack = 48;
+
+__device__ __forceinline__ double pinf() { return __longlong_as_double(0x7ff0000000000000LL); }
+
+// ------------------------------------------------------------------ sinks
+// Fused reduction in segment order (src/reduction.cpp:8-83).  NF > 0: the
+// field count known at compile time, accumulators in registers; NF == 0: any
+// count, accumulated in place in the output row.
+template <int MODE, int NF>
+struct Reducer {
+  const DevCloud* c;
+  double* row;
+  double acc[NF > 0 ? NF : 3];
+  double T;
+  unsigned nseg;
+  __device__ __forceinline__ void init(const DevCloud* cc, double* r) {
+    c = cc;
+    row = r;
+    nseg = 0;
+    T = 1.0;
+    const double init = MODE == kMax ? -pinf() : (MODE == kMin ? pinf() : 0.0);
+    if (MODE == kVolume) {
+      acc[0] = acc[1] = acc[2] = 0.0;
+    } else if (NF > 0) {
+#pragma unroll
+      for (int f = 0; f < (NF > 0 ? NF : 1); ++f) acc[f] = init;
+    } else {
+      for (int f = 0; f < c->nf; ++f) row[f] = init;
+    }
+  }
+  __device__ __forceinline__ void seg(int cell, double a, double b) {
+    ++nseg;
+    const int nf = NF > 0 ? NF : c->nf;
+    const double* F = c->fields + (int64_t)cell * nf;
+    if (MODE == kVolume) {
+      // reduce_volume_render (src/reduction.cpp:68-80)
+      const double alpha = F[3];
+      const double ds = dsub(b, a);
+      const double opac = dsub(1.0, exp(dmul(-alpha, ds)));
+#pragma unroll
+      for (int k = 0; k < 3; ++k) acc[k] = dadd(acc[k], dmul(dmul(T, F[k]), opac));
+      T = dmul(T, dsub(1.0, opac));
+    } else if (NF > 0) {
+      const double ds = dsub(b, a);
+#pragma unroll
+      for (int f = 0; f < (NF > 0 ? NF : 1); ++f) {
+        const double v = F[f];
+        if (MODE == kSum) acc[f] = dadd(acc[f], dmul(ds, v));
+        else if (MODE == kMax) acc[f] = v > acc[f] ? v : acc[f];
+        else acc[f] = v < acc[f] ? v : acc[f];
+      }
+    } else {
+      const double ds = dsub(b, a);
+      for (int f = 0; f < nf; ++f) {
+        const double v = F[f];
+        if (MODE == kSum) row[f] = dadd(row[f], dmul(ds, v));
+        else if (MODE == kMax) row[f] = v > row[f] ? v : row[f];
+        else row[f] = v < row[f] ? v : row[f];
+      }
+    }
+  }
+  __device__ __forceinline__ void write(double* out) const {
+    if (MODE == kVolume) {
+      out[0] = acc[0];
+      out[1] = acc[1];
+      out[2] = acc[2];
+    } else if (NF > 0) {
+#pragma unroll
+      for (int f = 0; f < (NF > 0 ? NF : 1); ++f) out[f] = acc[f];
+    }
+  }
+};
+
+// CSR segment writer (src/projection.cpp:221-238): internal ids via perm.
+struct FillSink {
+  const DevCloud* c;
+  int64_t* cell;
+  double* se;
+  double* sx;
+  int64_t off;
+  unsigned nseg;
+  __device__ __forceinline__ void init(const DevCloud* cc, const WalkIO& io, int64_t ray) {
+    c = cc;
+    cell = io.seg_cell;
+    se = io.seg_enter;
+    sx = io.seg_exit;
+    off = io.offsets[ray];
+    nseg = 0;
+  }
+  __device__ __forceinline__ void seg(int cl, double a, double b) {
+    const int64_t k = off + nseg;
+    cell[k] = c->perm[cl];
+    se[k] = a;
+    sx[k] = b;
+    ++nseg;
+  }
+};
+
+// Adjoint of the reductions w.r.t. the per-cell fields.  The first `skip`
+// segments were already scattered by an earlier, handed-over launch.
+//   SUM:    g[c,f] += gbar[f] * ds
+//   VOLUME: o = 1 - exp(-alpha ds), T transmittance before the segment,
+//           S = sum of later contributions = C - (prefix incl. this one)
+//           d/d rgb_k   = gbar_k T o
+//           d/d alpha   = ds * sum_k gbar_k (T rgb_k (1 - o) - S_k)
+template <int MODE, int NF>
+struct AdjSink {
+  const DevCloud* c;
+  double* grad;
+  const double* grow;  // upstream gradient row
+  double g[NF > 0 ? NF : 3];
+  double C[3], P[3];
+  double T;
+  unsigned nseg, skip;
+  __device__ __forceinline__ void init(const DevCloud* cc, const WalkIO& io, int64_t ray,
+                                       unsigned sk) {
+    c = cc;
+    grad = io.grad;
+    grow = io.gout + ray * io.nout;
+    skip = sk;
+    nseg = 0;
+    T = 1.0;
+    if (MODE == kVolume) {
+      for (int k = 0; k < 3; ++k) {
+        g[k] = grow[k];
+        C[k] = io.fwd[ray * 3 + k];
+        P[k] = 0.0;
+      }
+    } else if (NF > 0) {
+#pragma unroll
+      for (int f = 0; f < (NF > 0 ? NF : 1); ++f) g[f] = grow[f];
+    }
+  }
+  __device__ __forceinline__ void seg(int cell, double a, double b) {
+    const bool emit = nseg >= skip;
+    ++nseg;
+    const double ds = dsub(b, a);
+    const int nf = NF > 0 ? NF : c->nf;
+    const int64_t pid = c->perm[cell];
+    if (MODE == kVolume) {
+      const double* F = c->fields + (int64_t)cell * 4;
+      const double alpha = F[3];
+      const double e = exp(dmul(-alpha, ds));
+      const double o = dsub(1.0, e);
+      double galpha = 0.0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double contrib = dmul(dmul(T, F[k]), o);
+        P[k] = dadd(P[k], contrib);
+        const double S = C[k] - P[k];
+        galpha += g[k] * (T * F[k] * e - S);
+        if (emit) atomicAdd(&grad[pid * 4 + k], g[k] * T * o);
+      }
+      if (emit) atomicAdd(&grad[pid * 4 + 3], ds * galpha);
+      T = dmul(T, dsub(1.0, o));  // same rounding as the forward pass
+    } else if (NF > 0) {
+      if (emit) {
+#pragma unroll
+        for (int f = 0; f < (NF > 0 ? NF : 1); ++f) atomicAdd(&grad[pid * nf + f], g[f] * ds);
+      }
+    } else if (emit) {
+      for (int f = 0; f < nf; ++f) atomicAdd(&grad[pid * nf + f], grow[f] * ds);
+    }
+  }
+};
+
+struct NullSink {
+  unsigned nseg = 0;
+  __device__ __forceinline__ void seg(int, double, double) { ++nseg; }
+};
+
+// ------------------------------------------------------- per-ray driver
+template <int MODE, int NF, int OUT, class Srch, class Stack>
+__device__ __forceinline__ int run_ray(const DevCloud& c, const WalkIO& io, int64_t ray,
+                                       Srch& S, Stack& st, unsigned skip, unsigned& nseg) {
+  RayGeom g;
+  ray_init(g, io.starts + 3 * ray, io.ends + 3 * ray);
+  if (!ray_finite(g)) {
+    nseg = 0;
+    return kErrNonFinite;
+  }
+  int rc;
+  if (OUT == kOutImage || OUT == kOutCount) {
+    double* row = io.out + ray * io.nout;
+    Reducer<MODE, NF> red;
+    red.init(&c, row);
+    rc = walk_ray(c, g, io.max_iter, S, st, red, (WalkDiag*)nullptr);
+    nseg = red.nseg;
+    if (rc == 0) {
+      red.write(row);
+      if (OUT == kOutCount) io.counts[ray] = red.nseg;
+    }
+  } else if (OUT == kOutFill) {
+    FillSink fs;
+    fs.init(&c, io, ray);
+    rc = walk_ray(c, g, io.max_iter, S, st, fs, (WalkDiag*)nullptr);
+    nseg = fs.nseg;
+  } else {
+    AdjSink<MODE, NF> as;
+    as.init(&c, io, ray, skip);
+    rc = walk_ray(c, g, io.max_iter, S, st, as, (WalkDiag*)nullptr);
+    nseg = as.nseg;
+  }
+  return rc;
+}
+
+__device__ __forceinline__ void report(const WalkIO& io, int64_t ray, int rc) {
+  if (rc && rc != kNeedSlow)
+    atomicMin(&io.stats->first_error, ((unsigned long long)ray << 8) | (unsigned)rc);
+}
+
+__device__ __forceinline__ void hand_over(const WalkIO& io, int64_t ray, unsigned emitted) {
+  const unsigned long long k = atomicAdd(&io.stats->slow_count, 1ULL);
+  io.slow_q[k] = ((unsigned long long)ray << 24) | (emitted & 0xffffffu);
+}
+
+// ------------------------------------------------------------ k_plain
+template <int MODE, int NF, int OUT>
+__global__ void __launch_bounds__(128) k_plain(DevCloud c, WalkIO io) {
+  const int64_t ray = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (ray >= io.nrays) return;
+  Search64 S(c);
+  LocalStack<kPlainStack> st;
+  st.clear();
+  unsigned nseg = 0;
+  int rc = run_ray<MODE, NF, OUT>(c, io, ray, S, st, 0u, nseg);
+  if (rc == kNeedSlow) hand_over(io, ray, nseg);
+  report(io, ray, rc);
+  warp_add(&io.stats->rays, 1u);
+  warp_add(&io.stats->crossings, rc == 0 ? nseg : 0u);
+  warp_add(&io.stats->queries, S.nq);
+  warp_max(&io.stats->max_stack, (unsigned)st.maxsp);
+}
+
+// ------------------------------------------------------------- k_slow
+template <int MODE, int NF, int OUT>
+__global__ void __launch_bounds__(128) k_slow(DevCloud c, WalkIO io) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  GlobalStack st;
+  st.id = io.gstack_id + (int64_t)tid * io.gstack_cap;
+  st.s = io.gstack_s + (int64_t)tid * io.gstack_cap;
+  st.cap = io.gstack_cap;
+  st.clear();
+  const unsigned long long total = io.stats->slow_count;
+  for (unsigned long long q = tid; q < total; q += io.slow_threads) {
+    const unsigned long long e = io.slow_q[q];
+    const int64_t ray = (int64_t)(e >> 24);
+    const unsigned skip = (unsigned)(e & 0xffffffu);
+    Search64 S(c);
+    unsigned nseg = 0;
+    int rc = run_ray<MODE, NF, OUT>(c, io, ray, S, st, skip, nseg);
+    if (rc == kNeedSlow) rc = kErrStack;
+    report(io, ray, rc);
+    atomicAdd(&io.stats->slow_rays, 1ULL);
+    if (rc == 0) atomicAdd(&io.stats->crossings, (unsigned long long)nseg);
+    atomicAdd(&io.stats->queries, (unsigned long long)S.nq);
+    atomicMax(&io.stats->max_stack, (unsigned long long)st.maxsp);
+  }
+}
+
+// ------------------------------------------------------------- k_diag
+__global__ void k_diag(DevCloud c, WalkIO io, int64_t ray) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  GlobalStack st;
+  st.id = io.gstack_id;
+  st.s = io.gstack_s;
+  st.cap = io.gstack_cap;
+  RayGeom g;
+  ray_init(g, io.starts + 3 * ray, io.ends + 3 * ray);
+  Search64 S(c);
+  NullSink ns;
+  io.diag->code = 0;
+  int rc = walk_ray(c, g, io.max_iter, S, st, ns, io.diag);
+  if (rc == kNeedSlow) rc = kErrStack;
+  io.diag->code = rc;
+  if (rc) {
+    io.diag->c = io.diag->c >= 0 ? c.perm[io.diag->c] : -1;
+    io.diag->n = io.diag->n >= 0 ? c.perm[io.diag->n] : -1;
+  }
+}
+
+// -------------------------------------------------------------- k_knn
+__global__ void k_knn(DevCloud c, const double* __restrict__ q, int64_t nq, int k, int64_t* ids,
+                      double* r2) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  KnnBig<128> r;
+  r.clear(k);
+  unsigned v = 0;
+  knn_exact64(c, q[3 * i], q[3 * i + 1], q[3 * i + 2], pinf(), r, v);
+  for (int j = 0; j < k; ++j) {
+    const bool ok = j < r.cnt;
+    ids[i * k + j] = ok ? (int64_t)c.perm[r.id[j]] : -1;
+    r2[i * k + j] = ok ? r.r2[j] : DBL_MAX;
+  }
+}
+
+}  // namespace vt
+
+// batched kernel (persistent, guarded FP32)
+#include "batched.cuh"
+
+namespace vt {
+
+// ------------------------------------------------------------ dispatch
+template <int MODE, int NF, int OUT>
+static int launch_walk_t(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) {
+  const DevCloud& c = cl->view;
+  if (io.nrays > 0) {
+    if (kernel == VT_KERNEL_PLAIN_FP64) {
+      const int B = 128;
+      k_plain<MODE, NF, OUT><<<(unsigned)((io.nrays + B - 1) / B), B, 0, st>>>(c, io);
+    } else {
+      int rc = launch_batched<MODE, NF, OUT>(cl, io, kernel, st);
+      if (rc) return rc;
+    }
+    VT_CUDA(cudaGetLastError());
+    const int SB = 128;
+    k_slow<MODE, NF, OUT><<<(unsigned)(io.slow_threads / SB), SB, 0, st>>>(c, io);
+    VT_CUDA(cudaGetLastError());
+  }
+  return VT_OK;
+}
+
+template <int OUT>
+static int launch_walk_mode(vt_cloud* cl, WalkIO& io, int mode, int kernel, cudaStream_t st) {
+  const int nf = (int)cl->nfields;
+  switch (mode) {
+    case kSum:
+      if (nf == 1) return launch_walk_t<kSum, 1, OUT>(cl, io, kernel, st);
+      if (nf == 3) return launch_walk_t<kSum, 3, OUT>(cl, io, kernel, st);
+      if (nf == 4) return launch_walk_t<kSum, 4, OUT>(cl, io, kernel, st);
+      return launch_walk_t<kSum, 0, OUT>(cl, io, kernel, st);
+    case kVolume:
+      return launch_walk_t<kVolume, 4, OUT>(cl, io, kernel, st);
+    default:
+      break;
+  }
+  if (OUT == kOutAdj) return set_error(VT_ERR_INVALID, "adjoint is defined for 'integrate' and 'volume' only");
+  if (mode == kMax) {
+    if (nf == 1) return launch_walk_t<kMax, 1, (OUT == kOutAdj ? kOutImage : OUT)>(cl, io, kernel, st);
+    return launch_walk_t<kMax, 0, (OUT == kOutAdj ? kOutImage : OUT)>(cl, io, kernel, st);
+  }
+  if (nf == 1) return launch_walk_t<kMin, 1, (OUT == kOutAdj ? kOutImage : OUT)>(cl, io, kernel, st);
+  return launch_walk_t<kMin, 0, (OUT == kOutAdj ? kOutImage : OUT)>(cl, io, kernel, st);
+}
+
+static std::string fmt_double(double v) {
+  // std::to_string(double) formatting ("%f"), as in the reference's message
+  char buf[64];
+  snprintf(buf, sizeof(buf), "%f", v);
+  return buf;
+}
+
+// Run one walk launch (+ handed-over rays) and turn a per-ray failure into
+// the reference's error message.
+int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaStream_t st,
+             vt_stats* stats) {
+  const int slow_threads = 1024;
+  if (cl->ws_stats.reserve(1)) return VT_ERR_NOMEM;
+  if (cl->ws_slow.reserve(io.nrays > 0 ? io.nrays : 1)) return VT_ERR_NOMEM;
+  if (cl->ws_stack_id.reserve((size_t)slow_threads * cl->stack_cap)) return VT_ERR_NOMEM;
+  if (cl->ws_stack_s.reserve((size_t)slow_threads * cl->stack_cap)) return VT_ERR_NOMEM;
+  io.stats = cl->ws_stats.p;
+  io.slow_q = cl->ws_slow.p;
+  io.gstack_id = cl->ws_stack_id.p;
+  io.gstack_s = cl->ws_stack_s.p;
+  io.gstack_cap = cl->stack_cap;
+  io.slow_threads = slow_threads;
+  io.max_iter = cl->max_iter;
+  io.diag = nullptr;
+  VT_CUDA(cudaMemsetAsync(io.stats, 0, sizeof(DevStats), st));
+  VT_CUDA(cudaMemsetAsync(&io.stats->first_error, 0xff, sizeof(unsigned long long), st));
+  cudaEvent_t e0, e1;
+  VT_CUDA(cudaEventCreate(&e0));
+  VT_CUDA(cudaEventCreate(&e1));
+  VT_CUDA(cudaEventRecord(e0, st));
+  int rc;
+  switch (out_kind) {
+    case kOutImage: rc = launch_walk_mode<kOutImage>(cl, io, mode, kernel, st); break;
+    case kOutCount: rc = launch_walk_mode<kOutCount>(cl, io, mode, kernel, st); break;
+    case kOutFill: rc = launch_walk_t<kSum, 1, kOutFill>(cl, io, kernel, st); break;
+    default: rc = launch_walk_mode<kOutAdj>(cl, io, mode, kernel, st); break;
+  }
+  if (rc) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+  }
+  VT_CUDA(cudaEventRecord(e1, st));
+  DevStats hs;
+  VT_CUDA(cudaMemcpyAsync(&hs, io.stats, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (stats) {
+    stats->rays = hs.rays;
+    stats->crossings = hs.crossings;
+    stats->queries = hs.queries;
+    stats->fp64_resolves = hs.fp64_resolves;
+    stats->slow_rays = hs.slow_rays;
+    stats->max_stack = hs.max_stack;
+    stats->walk_ms = ms;
+  }
+  if (hs.first_error != ~0ULL) {
+    const int64_t ray = (int64_t)(hs.first_error >> 8);
+    const int code = (int)(hs.first_error & 0xff);
+    // re-walk the failing ray alone for the message details
+    DevBuf<WalkDiag> dg;
+    if (dg.alloc(1)) return VT_ERR_NOMEM;
+    WalkDiag hd{0, -1, -1, 0.0, 0.0, 0.0};
+    VT_CUDA(cudaMemcpyAsync(dg.p, &hd, sizeof(hd), cudaMemcpyHostToDevice, st));
+    io.diag = dg.p;
+    k_diag<<<1, 1, 0, st>>>(cl->view, io, ray);
+    VT_CUDA(cudaGetLastError());
+    VT_CUDA(cudaMemcpyAsync(&hd, dg.p, sizeof(hd), cudaMemcpyDeviceToHost, st));
+    VT_CUDA(cudaStreamSynchronize(st));
+    io.diag = nullptr;
+    std::string msg;
+    switch (code) {
+      case kErrMaxIter: msg = "Ray walk exceeded maximum iteration count"; break;
+      case kErrSplitBounds:
+        msg = "Split point outside segment bounds: s=" + fmt_double(hd.s) + " not in (" +
+              fmt_double(hd.s_lo) + ", " + fmt_double(hd.s_hi) + ") for cells " +
+              std::to_string(hd.c) + " and " + std::to_string(hd.n);
+        break;
+      case kErrBinSearch:
+        msg = "Binary search did not converge for split point between cells " +
+              std::to_string(hd.c) + " and " + std::to_string(hd.n);
+        break;
+      case kErrPerturb:
+        msg = "Perturbation did not resolve degenerate split point after " +
+              std::to_string(kMaxPerturbCycles) + " cycles";
+        break;
+      case kErrKnnExpand:
+        msg = "Could not resolve split point classification after expanding to " +
+              std::to_string(kExpandK) +
+              "-NN. This should be very unlikely; consider increasing TOLERANCE or K_EXPAND.";
+        break;
+      case kErrStack:
+        msg = "Ray walk exceeded the pending-point stack capacity (" +
+              std::to_string(cl->stack_cap) + ")";
+        break;
+      case kErrNonFinite: msg = "Ray endpoints must be finite"; return set_error(VT_ERR_INVALID, msg + " (ray " + std::to_string(ray) + ")");
+      default: msg = "ray walk failed with code " + std::to_string(code); break;
+    }
+    return set_error(code, msg);
+  }
+  return VT_OK;
+}
+
+int run_knn(vt_cloud* cl, const double* d_q, int64_t nq, int k, int64_t* d_ids, double* d_r2,
+            cudaStream_t st) {
+  const int B = 128;
+  if (nq > 0) k_knn<<<(unsigned)((nq + B - 1) / B), B, 0, st>>>(cl->view, d_q, nq, k, d_ids, d_r2);
+  VT_CUDA(cudaGetLastError());
+  return VT_OK;
+}
+
+// exclusive prefix sum of counts[0..n) into offsets[0..n]
+int scan_offsets(vt_cloud* cl, const int64_t* d_counts, int64_t* d_offsets, int64_t n,
+                 cudaStream_t st) {
+  size_t bytes = 0;
+  VT_CUDA(cub::DeviceScan::InclusiveSum(nullptr, bytes, d_counts, d_offsets + 1, (int)n, st));
+  if (cl->ws_tmp.reserve(bytes)) return VT_ERR_NOMEM;
+  VT_CUDA(cudaMemsetAsync(d_offsets, 0, sizeof(int64_t), st));
+  if (n > 0)
+    VT_CUDA(cub::DeviceScan::InclusiveSum(cl->ws_tmp.p, bytes, d_counts, d_offsets + 1, (int)n, st));
+  return VT_OK;
+}
+
+}  // namespace vt

@@ -1,0 +1,46 @@
+// walkio.h -- arguments of one walk launch (shared by the kernels in
+// project.cu and the host entry points in api.cu).
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/vortrace_b200.h"
+#include "common.cuh"
+
+struct vt_cloud;
+
+namespace vt {
+
+constexpr int kOutImage = 0, kOutCount = 1, kOutFill = 2, kOutAdj = 3;
+constexpr int kErrNonFinite = 16;
+
+struct WalkDiag;
+
+struct WalkIO {
+  const double* starts;  // nrays x 3, device
+  const double* ends;    // nrays x 3, device
+  int64_t nrays;
+  int nout;              // values per ray (3 for volume, else nfields)
+  double* out;           // image: nrays x nout
+  int64_t* counts;       // count: segments per ray
+  const int64_t* offsets;  // fill: CSR offsets
+  int64_t* seg_cell;
+  double* seg_enter;
+  double* seg_exit;
+  const double* gout;    // adjoint: upstream gradient, nrays x nout
+  const double* fwd;     // adjoint: forward output (volume)
+  double* grad;          // adjoint: npart x nfields, accumulated
+  DevStats* stats;
+  unsigned long long* slow_q;  // handed-over rays: (ray << 24) | segments emitted
+  int* gstack_id;              // global pending-point stacks of k_slow
+  double* gstack_s;
+  int gstack_cap;
+  int slow_threads;
+  int64_t max_iter;
+  WalkDiag* diag;
+};
+
+int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaStream_t st,
+             vt_stats* stats);
+
+}  // namespace vt

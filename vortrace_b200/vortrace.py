@@ -1,0 +1,353 @@
+"""High-level interface: :class:`ProjectionCloud`, a drop-in for the
+reference's ``vortrace.ProjectionCloud`` (vortrace/vortrace.py:24-419).
+
+Same constructor, methods, argument handling, output shapes and exceptions
+as the reference; the work runs in libvortrace_b200.so (C ABI, ctypes) on a
+B200.  Extras that do not change the reference's calls:
+  * ``kernel`` attribute: ``'auto'`` (batched guarded-FP32 kernel),
+    ``'plain'`` (one ray per thread, FP64), ``'batched'``, ``'batched_fp64'``;
+  * ``last_stats``: counters of the last projection (rays, crossings,
+    queries, FP64 re-resolves, handed-over rays, walk time);
+  * :meth:`batch_projection`: many grids and arbitrary rays in one launch.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import logging
+
+import numpy as np
+
+from . import _lib as L
+from . import grid as gr
+
+_log = logging.getLogger("vortrace")
+
+_REDUCTIONS = {
+    "integrate": L.REDUCE_SUM,
+    "sum": L.REDUCE_SUM,
+    "max": L.REDUCE_MAX,
+    "min": L.REDUCE_MIN,
+    "volume": L.REDUCE_VOLUME,
+}
+
+
+class _Cloud:
+    """Owning wrapper of a ``vt_cloud`` handle (the reference's PointCloud)."""
+
+    def __init__(self):
+        self._lib = L.load()
+        self._h = C.c_void_p()
+
+    def loadPoints(self, pos, fields, subbox, vol=None, periodic=False):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        fields = np.ascontiguousarray(fields, dtype=np.float64)
+        if pos.ndim != 2:
+            raise ValueError("pos array must be two-dimensional")
+        if fields.ndim == 1:
+            nf, nfp = 1, fields.shape[0]
+        elif fields.ndim == 2:
+            nf, nfp = fields.shape[1], fields.shape[0]
+        else:
+            raise ValueError("fields array must be one-dimensional or two-dimensional")
+        if pos.shape[0] != nfp:
+            raise ValueError(f"Input sizes must match: pos has {pos.shape[0]} rows but fields "
+                             f"has {nfp}")
+        sb = np.ascontiguousarray(np.asarray(subbox, dtype=np.float64).ravel())
+        if sb.size != 6:
+            raise ValueError("subbox must have 6 values")
+        v = None if vol is None else np.ascontiguousarray(vol, dtype=np.float64).ravel()
+        self.destroy()
+        L.check(self._lib.vt_cloud_create(L.dptr(pos), pos.shape[0], L.dptr(fields), nfp, nf,
+                                          L.dptr(sb), L.dptr(v), 0 if v is None else v.size,
+                                          int(bool(periodic)), C.byref(self._h)))
+
+    def buildTree(self):
+        L.check(self._lib.vt_cloud_build_tree(self._h))
+
+    def info(self) -> L.CloudInfo:
+        inf = L.CloudInfo()
+        L.check(self._lib.vt_cloud_get_info(self._h, C.byref(inf)))
+        return inf
+
+    def get_npart(self):
+        return self.info().npart
+
+    def get_nfields(self):
+        return self.info().nfields
+
+    def get_pad(self):
+        return self.info().pad
+
+    def get_valid_rgba(self):
+        return bool(self.info().valid_rgba)
+
+    def get_tree_built(self):
+        return bool(self.info().tree_built)
+
+    def get_periodic(self):
+        return bool(self.info().periodic)
+
+    def get_orig_ids(self):
+        n = self.get_npart()
+        out = np.empty(n, np.int64)
+        L.check(self._lib.vt_cloud_orig_ids(self._h, L.i64ptr(out), n))
+        return out
+
+    def set_param(self, param, value):
+        L.check(self._lib.vt_cloud_set_param(self._h, param, int(value)))
+
+    def queryTree(self, q, k=None):
+        """PointCloud.queryTree (src/bindings.cpp:155-174): nearest id, or
+        (ids, r2) arrays for k neighbours; ids are internal indices."""
+        qa = np.ascontiguousarray(np.asarray(q, np.float64).reshape(-1, 3))
+        kk = 1 if k is None else int(k)
+        ids = np.empty((qa.shape[0], kk), np.int64)
+        r2 = np.empty((qa.shape[0], kk), np.float64)
+        L.check(self._lib.vt_knn(self._h, L.dptr(qa), qa.shape[0], kk, L.i64ptr(ids),
+                                 L.dptr(r2)))
+        if k is None:
+            return int(ids[0, 0])
+        return ids[0], r2[0]
+
+    def knn(self, q, k):
+        qa = np.ascontiguousarray(np.asarray(q, np.float64).reshape(-1, 3))
+        ids = np.empty((qa.shape[0], k), np.int64)
+        r2 = np.empty((qa.shape[0], k), np.float64)
+        L.check(self._lib.vt_knn(self._h, L.dptr(qa), qa.shape[0], k, L.i64ptr(ids),
+                                 L.dptr(r2)))
+        return ids, r2
+
+    def destroy(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.vt_cloud_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def _project(cloud: _Cloud, starts, ends, mode, kernel, nout):
+    """Projection(starts, ends).makeProjection(cloud, mode) + returnProjection."""
+    n = starts.shape[0]
+    out = np.empty((n, nout), np.float64)
+    st = L.Stats()
+    L.check(cloud._lib.vt_project(cloud._h, L.dptr(starts), L.dptr(ends), n, mode,
+                                  L.KERNELS[kernel], L.dptr(out), C.byref(st)))
+    return out, st
+
+
+def _project_detailed(cloud: _Cloud, starts, ends, mode, nout):
+    n = starts.shape[0]
+    out = np.empty((n, nout), np.float64)
+    offsets = np.empty(n + 1, np.int64)
+    seg = C.c_void_p()
+    lib = cloud._lib
+    L.check(lib.vt_project_detailed(cloud._h, L.dptr(starts), L.dptr(ends), n, mode,
+                                    L.dptr(out), L.i64ptr(offsets), C.byref(seg)))
+    try:
+        tot = lib.vt_segments_count(seg)
+        cid = np.empty(tot, np.int64)
+        se = np.empty(tot, np.float64)
+        sx = np.empty(tot, np.float64)
+        L.check(lib.vt_segments_copy(seg, L.i64ptr(cid), L.dptr(se), L.dptr(sx)))
+    finally:
+        lib.vt_segments_free(seg)
+    return out, cid, se, sx, offsets
+
+
+def _as_values(out, nout):
+    """returnProjection shape: (n,) for one value per ray, else (n, nout)."""
+    return out[:, 0].copy() if nout == 1 else out
+
+
+class ProjectionCloud:
+    """Projections through an unstructured Voronoi mesh on a B200.
+
+    Same interface as the reference's ``vortrace.ProjectionCloud``.
+    """
+
+    _REDUCTION_MAP = dict(_REDUCTIONS)
+
+    def __init__(self, pos, fields, boundbox=None, vol=None, *, periodic: bool = False,
+                 _skip_build_tree: bool = False) -> None:
+        self.pos_orig = np.ascontiguousarray(pos, dtype=np.float64)
+        self.fields_orig = np.ascontiguousarray(fields, dtype=np.float64)
+        self.vol_orig = (np.ascontiguousarray(vol, dtype=np.float64)
+                         if vol is not None else None)
+        self.periodic = periodic
+        fa = self.fields_orig
+        if fa.ndim == 1:
+            self._nfields = 1
+        elif fa.ndim == 2:
+            self._nfields = fa.shape[1]
+        else:
+            raise ValueError("fields must be 1D (npart,) or 2D (npart, nfields)")
+        if boundbox is None:
+            boundbox = [pos[:, 0].min(), pos[:, 0].max(), pos[:, 1].min(), pos[:, 1].max(),
+                        pos[:, 2].min(), pos[:, 2].max()]
+        self.boundbox = boundbox
+        self.kernel = "auto"
+        self.last_stats = None
+        self._cloud = _Cloud()
+        self._cloud.loadPoints(self.pos_orig, self.fields_orig, boundbox, self.vol_orig,
+                               periodic)
+        if not _skip_build_tree:
+            self._cloud.buildTree()
+        self.orig_ids = np.array(self._cloud.get_orig_ids())
+        _log.info("Applied bounding box filter: %d -> %d particles", len(self.pos_orig),
+                  len(self.orig_ids))
+
+    # -------------------------------------------------------------- helpers
+    def _validate_reduction(self, reduction: str) -> int:
+        mode = self._REDUCTION_MAP.get(reduction)
+        if mode is None:
+            raise ValueError(f"Unknown reduction {reduction!r}. "
+                             f"Use one of {list(self._REDUCTION_MAP)}")
+        if mode == L.REDUCE_VOLUME:
+            if self._nfields != 4:
+                raise ValueError("Volume rendering requires exactly 4 fields "
+                                 f"(R, G, B, alpha), got {self._nfields}")
+            if not self._cloud.get_valid_rgba():
+                raise ValueError("Volume rendering requires R, G, B values in [0, 1] "
+                                 "and alpha >= 0")
+        return mode
+
+    def _prepare_array_for_backend(self, arr) -> np.ndarray:
+        a = np.asarray(arr)
+        if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+            a = np.ascontiguousarray(a, dtype=np.float64)
+        return a
+
+    def _nout(self, mode):
+        return 3 if mode == L.REDUCE_VOLUME else self._nfields
+
+    def _run(self, starts, ends, mode):
+        if starts.shape[0] == 0:
+            # the reference's returnProjection on an empty result
+            raise RuntimeError("Projection has not yet been made")
+        out, st = _project(self._cloud, starts, ends, mode, self.kernel, self._nout(mode))
+        self.last_stats = st.as_dict()
+        return out
+
+    # ----------------------------------------------------------- projections
+    def grid_projection(self, extent, nres, bounds, center, *, proj=None, yaw=0.0, pitch=0.0,
+                        roll=0.0, reduction="integrate") -> np.ndarray:
+        """Grid projection; see the reference (vortrace/vortrace.py:141-195)."""
+        mode = self._validate_reduction(reduction)
+        ps, pe = gr.generate_projection_grid(extent, nres, bounds, center, proj=proj, yaw=yaw,
+                                             pitch=pitch, roll=roll)
+        shape = ps.shape
+        ps = np.ascontiguousarray(ps.reshape(-1, shape[-1]))
+        pe = np.ascontiguousarray(pe.reshape(-1, pe.shape[-1]))
+        dat = self._run(ps, pe, mode)
+        nout = self._nout(mode)
+        if nout == 1:
+            return np.reshape(dat, shape[:-1])
+        return np.reshape(dat, (*shape[:-1], nout))
+
+    def projection(self, pos_start, pos_end, *, reduction="integrate") -> np.ndarray:
+        """Projection of arbitrary rays (vortrace/vortrace.py:197-227)."""
+        mode = self._validate_reduction(reduction)
+        pos_start = self._prepare_array_for_backend(pos_start)
+        pos_end = self._prepare_array_for_backend(pos_end)
+        if (pos_start.ndim != 2 or pos_end.ndim != 2 or pos_start.shape != pos_end.shape
+                or pos_start.shape[1] != 3):
+            raise ValueError("pos_start / pos_end must be 2D arrays of identical shape (N,3)")
+        out = self._run(pos_start, pos_end, mode)
+        return _as_values(out, self._nout(mode))
+
+    def traced_projection(self, pos_start, pos_end, return_midpoint: bool = True, *,
+                          reduction: str = "integrate", flatten: bool = False) -> tuple:
+        """Projection with per-segment detail (vortrace/vortrace.py:229-338)."""
+        ps = np.asarray(pos_start)
+        pe = np.asarray(pos_end)
+        single = False
+        if ps.ndim == 1 and pe.ndim == 1:
+            if ps.shape != (3,) or pe.shape != (3,):
+                raise ValueError("If 1D, pos_start and pos_end must both have shape (3,)")
+            ps = ps[np.newaxis, :]
+            pe = pe[np.newaxis, :]
+            single = True
+        elif ps.ndim == 2 and pe.ndim == 2:
+            if ps.shape != pe.shape or ps.shape[1] != 3:
+                raise ValueError("pos_start and pos_end must be 2D arrays of identical shape "
+                                 "(N, 3)")
+            if ps.shape[0] == 1:
+                single = True
+        else:
+            raise ValueError("pos_start and pos_end must both be 1D shape (3,) or both 2D "
+                             "shape (N, 3)")
+        ps = self._prepare_array_for_backend(ps)
+        pe = self._prepare_array_for_backend(pe)
+        mode = self._validate_reduction(reduction)
+        nout = self._nout(mode)
+        if ps.shape[0] == 0:
+            raise RuntimeError("Projection has not yet been made")
+        out, cid, se, sx, offsets = _project_detailed(self._cloud, ps, pe, mode, nout)
+        values = _as_values(out, nout)
+        cell_ids = self.orig_ids[cid]
+        ds_vals = sx - se
+        s_vals = (se + sx) / 2.0 if return_midpoint else se
+        if single:
+            if mode == L.REDUCE_VOLUME or self._nfields > 1:
+                val_out = values[0]
+            else:
+                val_out = values[0] if values.ndim == 1 else values[0, 0]
+            return val_out, cell_ids, s_vals, ds_vals
+        if flatten:
+            return values, cell_ids, s_vals, ds_vals, offsets
+        nr = len(offsets) - 1
+        return (values, [cell_ids[offsets[i]:offsets[i + 1]] for i in range(nr)],
+                [s_vals[offsets[i]:offsets[i + 1]] for i in range(nr)],
+                [ds_vals[offsets[i]:offsets[i + 1]] for i in range(nr)])
+
+    def single_projection(self, *args, **kwargs):
+        """Removed.  Use :meth:`traced_projection` instead."""
+        raise AttributeError("'single_projection' has been removed. "
+                             "Use 'traced_projection' instead.")
+
+    def batch_projection(self, grids=(), rays=None, *, reduction="integrate"):
+        """Many projections in one launch (extension; not in the reference).
+
+        ``grids``: sequence of dicts with the keyword arguments of
+        :meth:`grid_projection` (``extent``, ``nres``, ``bounds``, ``center``
+        and optionally ``proj/yaw/pitch/roll``); ``rays``: optional
+        ``(pos_start, pos_end)`` arrays of arbitrary rays.  Returns a list of
+        images (one per grid) and, when ``rays`` is given, the ray values.
+        """
+        mode = self._validate_reduction(reduction)
+        starts, ends, shapes = [], [], []
+        for g in grids:
+            ps, pe = gr.generate_projection_grid(
+                g["extent"], g["nres"], g["bounds"], g.get("center"), proj=g.get("proj"),
+                yaw=g.get("yaw", 0.0), pitch=g.get("pitch", 0.0), roll=g.get("roll", 0.0))
+            shapes.append(ps.shape[:-1])
+            starts.append(ps.reshape(-1, 3))
+            ends.append(pe.reshape(-1, 3))
+        if rays is not None:
+            rs = self._prepare_array_for_backend(rays[0]).reshape(-1, 3)
+            re_ = self._prepare_array_for_backend(rays[1]).reshape(-1, 3)
+            starts.append(rs)
+            ends.append(re_)
+        S = np.ascontiguousarray(np.concatenate(starts)) if starts else np.empty((0, 3))
+        E = np.ascontiguousarray(np.concatenate(ends)) if ends else np.empty((0, 3))
+        out = self._run(S, E, mode)
+        nout = self._nout(mode)
+        imgs, o = [], 0
+        for sh in shapes:
+            k = int(np.prod(sh))
+            blk = out[o:o + k]
+            imgs.append(blk.reshape(sh) if nout == 1 else blk.reshape(*sh, nout))
+            o += k
+        if rays is not None:
+            return imgs, _as_values(out[o:], nout)
+        return imgs
+
+    # ------------------------------------------------------------- cloud
+    def query(self, q, k=1):
+        """Exact k nearest generators of query points (original ids, r^2)."""
+        ids, r2 = self._cloud.knn(q, k)
+        return np.where(ids >= 0, self.orig_ids[np.maximum(ids, 0)], -1), r2
