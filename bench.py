@@ -1,0 +1,444 @@
+#!/usr/bin/env python
+"""Benchmark of the exact Voronoi ray walk on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config clustered_2m]
+
+One step = one projection of the workload's rays through the cloud (the
+cloud and its device tree are built once, outside the timed region, as the
+reference's timing of Projection::makeProjection excludes buildTree).
+Prints one JSON line (rank 0).
+
+Metric: cell crossings per second (Mcrossings/s) of the batched guarded-FP32
+kernel, forward; the same line reports forward+adjoint and the plain FP64
+one-ray-per-thread kernel.  Multi-GPU (torchrun): every rank projects its own
+view of the cloud (the grid rotated about the cloud centre by 2*pi*rank/N):
+weak scaling, no data-path collective; value = all ranks' crossings / max
+over ranks of the timed device time.
+
+``--impl reference`` times the reference's own CPU implementation (its
+Cvortrace module compiled from its sources into oracle/_ref, OpenMP over all
+host cores; the C restatement in oracle/ when that module is absent) on a
+bounded sample of the same rays.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+import warnings
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcrossings/s fwd & fwd+bwd: batched guarded-FP32 vs plain FP64 GPU kernel"
+UNIT = "Mcrossings/s"
+# Algorithmic bytes per cell crossing, B_x = Q*(n_node*16 + n_pt*24) + nf*8 + 48,
+# measured with the nanoflann restatement (oracle/measure_bx.py, 8192-ray sample).
+BX = {"clustered_2m": 3262.25, "uniform_100k": 2915.74}
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.lines = []
+        self.proc = None
+        self.th = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.idx)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.th:
+            self.th.join(timeout=5)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = max(smax, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(name, rank, world, npix=None):
+    from vortrace_b200 import workloads as W
+    from vortrace_b200 import grid as gr
+    w = W.CONFIGS[name]() if not npix else W.CONFIGS[name](npix=npix)
+    if world > 1 and rank > 0:
+        # weak scaling: each rank projects its own view (rotated about the centre)
+        c = np.array([50.0, 50.0, 50.0])
+        R = gr.rotation_matrix(2 * np.pi * rank / world, 0.0, 0.0)
+        w["starts"] = np.ascontiguousarray((w["starts"] - c) @ R.T + c)
+        w["ends"] = np.ascontiguousarray((w["ends"] - c) @ R.T + c)
+    return w
+
+
+def cpu_reference_run(w, steps, nsample, warmup=0):
+    """Time the reference's own CPU path on a sample of the rays.
+
+    Returns (Mcrossings/s, crossings per step, seconds per step, kind,
+    rays in the sample)."""
+    from oracle import oracle as O
+    n = w["starts"].shape[0]
+    idx = np.linspace(0, n - 1, min(nsample, n)).astype(np.int64)
+    S = np.ascontiguousarray(w["starts"][idx])
+    E = np.ascontiguousarray(w["ends"][idx])
+    mod = O.load_reference_module()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        if mod is not None:
+            kind = "reference"
+            pc = mod.PointCloud()
+            pc.loadPoints(np.ascontiguousarray(w["pos"], np.float64),
+                          np.ascontiguousarray(w["fields"], np.float64), list(w["boundbox"]))
+            pc.buildTree()
+            mode = {"integrate": mod.ReductionMode.Sum,
+                    "volume": mod.ReductionMode.VolumeRender}[w["reduction"]]
+            pr = mod.Projection(S, E)
+            pr.makeDetailedProjection(pc, mode)
+            crossings = int(pr.returnSegments()[3][-1])
+
+            def step():
+                p = mod.Projection(S, E)
+                p.makeProjection(pc, mode)
+                return p.returnProjection()
+        else:
+            kind = "port"
+            lp = O.load_points(w["pos"], w["fields"], w["boundbox"])
+            t = O.OracleTree(lp["pts"], lp["fields"], lp["valid_rgba"])
+            _, segs = t.project(S, E, w["reduction"], segments=True)
+            crossings = int(segs[3][-1])
+
+            def step():
+                return t.project(S, E, w["reduction"])
+    for _ in range(warmup):
+        step()
+    times = []
+    for _ in range(max(1, steps)):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    sec = statistics.mean(times)
+    return crossings / sec / 1e6, crossings, sec, kind, len(idx)
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    w = make_workload(args.config, 0, 1)
+    val, cross, sec, kind, ns = cpu_reference_run(w, args.steps, args.cpu_sample,
+                                                  warmup=args.warmup)
+    cores = host_cores()
+    n = w["starts"].shape[0]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.config}: {w['meta']}",
+                   "sample": f"{ns} of {n} rays (evenly spaced)", "crossings_per_step": cross},
+        "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{ns} of {n} rays of {args.config}, OpenMP over all host "
+                                   "cores, tree build excluded"},
+        "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    import vortrace_b200 as vt
+    from vortrace_b200 import _lib as L
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    L.load().vt_set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    w = make_workload(args.config, rank, world, args.npix)
+    mode = {"integrate": L.REDUCE_SUM, "volume": L.REDUCE_VOLUME}[w["reduction"]]
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        pc = vt.ProjectionCloud(w["pos"], w["fields"], boundbox=w["boundbox"])
+    lib = pc._cloud._lib
+    h = pc._cloud._h
+    info = pc._cloud.info()
+    nf = int(info.nfields)
+    nout = 3 if mode == L.REDUCE_VOLUME else nf
+    S = np.ascontiguousarray(w["starts"])
+    E = np.ascontiguousarray(w["ends"])
+    n = S.shape[0]
+    d_s = torch.from_numpy(S).to(dev)
+    d_e = torch.from_numpy(E).to(dev)
+    d_out = torch.empty((n, nout), dtype=torch.float64, device=dev)
+    d_gout = torch.ones((n, nout), dtype=torch.float64, device=dev)
+    d_grad = torch.zeros((int(info.npart), nf), dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    st = L.Stats()
+
+    def fwd(kernel):
+        L.check(lib.vt_project_device(h, d_s.data_ptr(), d_e.data_ptr(), n, mode, kernel,
+                                      d_out.data_ptr(), stream.cuda_stream, C.byref(st)))
+        return st.crossings, st.walk_ms, st.fp64_resolves, st.queries
+
+    def bwd():
+        L.check(lib.vt_project_adjoint_device(h, d_s.data_ptr(), d_e.data_ptr(), n, mode,
+                                              d_out.data_ptr(), d_gout.data_ptr(),
+                                              d_grad.data_ptr(), stream.cuda_stream))
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def timed(fn, steps):
+        """Per-step device time (ms) with CUDA events on the launching stream;
+        L2 flushed before every step (outside the events)."""
+        ms = []
+        for i in range(steps):
+            flush.fill_(i & 0xff)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return ms
+
+    def reduce_max(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def reduce_sum(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    K, W = args.steps, args.warmup
+    # --- forward, batched guarded-FP32 kernel (the headline)
+    for _ in range(W):
+        fwd(L.KERNEL_BATCHED)
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    walk_ms = []
+
+    def f_b():
+        c, wm, _, _ = fwd(L.KERNEL_BATCHED)
+        walk_ms.append(wm)
+
+    fwd_ms = timed(f_b, K)
+    barrier()
+    clocks = sampler.stop()
+    crossings, _, resolves, queries = fwd(L.KERNEL_BATCHED)
+    t_fwd = reduce_max(sum(fwd_ms))
+    tot_cross = reduce_sum(float(crossings))
+    value = tot_cross * K / (t_fwd / 1e3) / 1e6
+
+    # --- forward + adjoint
+    for _ in range(max(1, W // 2)):
+        fwd(L.KERNEL_BATCHED)
+        bwd()
+    barrier()
+    fb_ms = timed(lambda: (fwd(L.KERNEL_BATCHED), bwd()), K)
+    barrier()
+    t_fb = reduce_max(sum(fb_ms))
+    fb_value = tot_cross * K / (t_fb / 1e3) / 1e6
+
+    # --- plain FP64 one-ray-per-thread kernel (the baseline kernel)
+    kp = max(2, K // 2)
+    fwd(L.KERNEL_PLAIN_FP64)
+    barrier()
+    pl_ms = timed(lambda: fwd(L.KERNEL_PLAIN_FP64), kp)
+    barrier()
+    t_pl = reduce_max(sum(pl_ms))
+    pl_value = tot_cross * kp / (t_pl / 1e3) / 1e6
+
+    # --- end to end through the C ABI with host buffers (pinned)
+    hS = torch.from_numpy(S).pin_memory().numpy()
+    hE = torch.from_numpy(E).pin_memory().numpy()
+    hO = torch.empty((n, nout), dtype=torch.float64).pin_memory().numpy()
+    st2 = L.Stats()
+
+    def e2e_step():
+        L.check(lib.vt_project(h, L.dptr(hS), L.dptr(hE), n, mode, L.KERNEL_AUTO, L.dptr(hO),
+                               C.byref(st2)))
+
+    e2e_step()
+    barrier()
+    e2e_s = []
+    for i in range(K):
+        flush.fill_(i & 0xff)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_s.append(time.perf_counter() - t0)
+    barrier()
+    t_e2e = reduce_max(sum(e2e_s))
+    e2e_value = tot_cross * K / t_e2e / 1e6
+
+    # --- roofline of the dominant kernel (k_batched + the tiny k_slow)
+    bx = BX.get(args.config)
+    peak, peak_src = None, None
+    mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(mp):
+        with open(mp) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    launch_ms = statistics.mean(walk_ms) if walk_ms else None
+    roof = None
+    if bx and launch_ms:
+        achieved = crossings * bx / (launch_ms / 1e3) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            with open(tp) as f:
+                tj = json.load(f).get(args.config)
+            if tj and tj.get("dram_bytes_per_crossing"):
+                traffic = float(tj["dram_bytes_per_crossing"]) * crossings
+        roof = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "peak_source": peak_src, "bytes_per_crossing": bx,
+                "kernel": "k_batched (guarded FP32)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            v, c, sec, kind, ns = cpu_reference_run(w, 2, args.cpu_sample)
+            cpu = {"value": round(v, 4), "unit": UNIT, "cores": host_cores(), "kind": kind,
+                   "sample": f"{ns} of {n} rays of {args.config} (evenly spaced), "
+                             f"{c} crossings, 2 steps, OpenMP over all host cores"}
+        except Exception as e:  # keep the GPU line even if the CPU leg fails
+            cpu = {"value": None, "unit": UNIT, "cores": host_cores(), "kind": "unavailable",
+                   "sample": f"CPU baseline failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": round(t_fwd / K, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{args.config}: {w['meta']}", "rays_per_gpu": n,
+                       "crossings_per_step": int(tot_cross), "reduction": w["reduction"],
+                       "l2": "flushed before every timed step (256 MB write)",
+                       "tree_build_ms": round(info.tree_build_ms, 2),
+                       "parallelism": f"rays sharded by view, {world} rank(s)"},
+            "fwd_bwd_mcrossings_per_s": round(fb_value, 4),
+            "plain_fp64_mcrossings_per_s": round(pl_value, 4),
+            "speedup_vs_plain_fp64": round(value / pl_value, 3),
+            "rays_per_s": round(n * world * K / (t_fwd / 1e3), 1),
+            "fp64_resolve_fraction": round(resolves / max(1, queries), 6),
+            "e2e": {"value": round(e2e_value, 4), "unit": UNIT,
+                    "h2d_bytes_per_step": int(2 * n * 3 * 8),
+                    "d2h_bytes_per_step": int(n * nout * 8)},
+            "gpu_launches": 2 * K,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="clustered_2m")
+    ap.add_argument("--cpu-sample", type=int, default=32768)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--npix", type=int, default=None,
+                    help="override the grid resolution (smaller profiling case)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

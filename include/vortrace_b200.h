@@ -62,6 +62,10 @@ extern "C" {
 #define VT_PARAM_SMEM_LEVELS 4    /* tree levels staged in shared memory       */
 #define VT_PARAM_BLOCKS_PER_SM 5  /* resident blocks per SM (0 = occupancy)    */
 #define VT_PARAM_LEAF_SIZE 6      /* max points per tree leaf (before build)   */
+#define VT_PARAM_LOCAL_STACK 7    /* pending points a ray may keep in the      */
+                                  /* kernels' in-register stack before it is   */
+                                  /* handed to the global-stack kernel         */
+                                  /* (default and maximum: the compiled size)  */
 
 typedef struct vt_cloud vt_cloud;
 typedef struct vt_segments vt_segments;
@@ -115,6 +119,13 @@ int vt_cloud_create(const double *pos, uint64_t npart, const double *fields,
 /* PointCloud::buildTree (src/pointcloud.cpp:193-212): device build. */
 int vt_cloud_build_tree(vt_cloud *cloud);
 int vt_cloud_set_param(vt_cloud *cloud, int param, int64_t value);
+/* Replace the per-point fields (npart x nfields, internal order, i.e. the
+ * order of vt_cloud_orig_ids) without rebuilding the tree, and re-check
+ * valid_rgba.  No reference counterpart (the reference reloads the points);
+ * used by the differentiable path.  The _device form takes a device pointer
+ * and a cudaStream_t (NULL: the handle's stream). */
+int vt_cloud_set_fields(vt_cloud *cloud, const double *fields);
+int vt_cloud_set_fields_device(vt_cloud *cloud, const double *d_fields, void *stream);
 /* PointCloud getters (src/bindings.cpp:134-154). */
 int vt_cloud_get_info(const vt_cloud *cloud, vt_cloud_info *info);
 /* PointCloud::get_orig_ids: writes min(cap, npart) ids. */

@@ -60,6 +60,7 @@ def lib():
         L.vto_knn.restype = C.c_size_t
         L.vto_knn.argtypes = [C.c_void_p, dp, C.c_size_t, szp, dp]
         L.vto_knn_batch.argtypes = [C.c_void_p, dp, C.c_size_t, C.c_size_t, i64p, dp]
+        L.vto_last_counters.argtypes = [C.POINTER(C.c_ulonglong)]
         L.vto_split_point_distance.restype = C.c_double
         L.vto_split_point_distance.argtypes = [dp, dp, dp, dp]
         L.vto_project.restype = C.c_int
@@ -227,6 +228,14 @@ class OracleTree:
                                _dp(se), _dp(sx), nthreads, _i64p(err_ray), msg, 512)
         self._check(rc, err_ray, msg)
         return out, (cid, se, sx, offsets)
+
+    @staticmethod
+    def last_counters():
+        """k-NN work of the last project() call: queries, nodes visited,
+        leaves visited, point distance evaluations."""
+        a = (C.c_ulonglong * 4)()
+        lib().vto_last_counters(a)
+        return {"queries": a[0], "nodes": a[1], "leaves": a[2], "points": a[3]}
 
     @staticmethod
     def _check(rc, err_ray, msg):

@@ -87,6 +87,13 @@ typedef struct {
 
 static inline double P(const vto_tree *t, size_t idx, int d) { return t->pts[idx * 3 + d]; }
 
+/* Work counters of the k-NN searches (per thread; summed by vto_project):
+ * queries, tree nodes visited (searchLevel calls), leaves visited, point
+ * distance evaluations.  They define the algorithmic bytes per crossing of
+ * the reference's own search (used for the roofline of the GPU kernels). */
+static __thread unsigned long long tl_cnt[4];
+static unsigned long long g_cnt[4];
+
 /* ------------------------------------------------------------------ build */
 
 static int64_t alloc_node(vto_tree *t) {
@@ -306,7 +313,10 @@ static inline double eval_metric(const vto_tree *t, const double *q, size_t idx)
 static void search_level(const vto_tree *t, vto_result *r, const double *vec, int64_t ni,
                          double mindistsq, double *dists) {
   const vto_node *node = &t->nodes[ni];
+  tl_cnt[1]++;
   if (node->child1 < 0 && node->child2 < 0) {
+    tl_cnt[2]++;
+    tl_cnt[3] += node->right - node->left;
     double wd = worst_dist(r);
     for (size_t i = node->left; i < node->right; ++i) {
       size_t index = t->vind[i];
@@ -346,6 +356,7 @@ size_t vto_knn(const vto_tree *t, const double *q, size_t k, size_t *ids, double
   vto_result r;
   result_init(&r, ids, r2, k);
   if (!t || t->n == 0 || k == 0) return 0;
+  tl_cnt[0]++;
   double dists[3] = {0.0, 0.0, 0.0};
   double distsq = 0.0;
   for (int i = 0; i < 3; ++i) {
@@ -711,6 +722,11 @@ static void reduce(const vto_ws *w, const double *fields, size_t nf, int mode, d
   }
 }
 
+/* counters of the last vto_project call: queries, nodes, leaves, points */
+void vto_last_counters(unsigned long long *out) {
+  for (int j = 0; j < 4; ++j) out[j] = g_cnt[j];
+}
+
 /*
  * Project nrays rays (src/projection.cpp:26-144).
  *   out:        nrays * nout values (nout = 3 for VOLUME, else nf)
@@ -746,10 +762,12 @@ int vto_project(const vto_tree *t, const double *fields, size_t nf, int valid_rg
 #else
   nthreads = 1;
 #endif
+  for (int j = 0; j < 4; ++j) g_cnt[j] = 0;
 #pragma omp parallel num_threads(nthreads)
   {
     vto_ws w;
     memset(&w, 0, sizeof(w));
+    for (int j = 0; j < 4; ++j) tl_cnt[j] = 0;
 #pragma omp for schedule(dynamic, 256)
     for (long long i = 0; i < (long long)nrays; ++i) {
       vto_ray r;
@@ -779,6 +797,10 @@ int vto_project(const vto_tree *t, const double *fields, size_t nf, int valid_rg
     }
     free(w.pts);
     free(w.segs);
+    for (int j = 0; j < 4; ++j) {
+#pragma omp atomic
+      g_cnt[j] += tl_cnt[j];
+    }
   }
   if (first_bad >= 0) {
     if (err_ray) *err_ray = first_bad;

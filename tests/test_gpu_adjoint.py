@@ -1,0 +1,196 @@
+"""Gradients of projections w.r.t. the per-cell fields (adjoint kernels).
+
+References:
+  * the sparse reference gradient A^T g, A[r, c] = sum of ds of ray r in cell
+    c, assembled from the oracle's segment lists (bit-identical to the
+    reference's makeDetailedProjection);
+  * for 'volume', the reverse-mode compositing adjoint evaluated in numpy on
+    those segment lists with exact suffix sums;
+  * central finite differences through the forward kernel (rtol 1e-6).
+"""
+import warnings
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import vortrace_b200 as vt
+from oracle import oracle as O
+from vortrace_b200 import _lib as L
+from vortrace_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FD_RTOL = 1e-6
+
+
+def setup(pos, fields, bb, starts, ends, mode):
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        pc = vt.ProjectionCloud(pos, fields, boundbox=bb)
+        lp = O.load_points(pos, fields, bb)
+    ot = O.OracleTree(lp["pts"], lp["fields"], lp["valid_rgba"])
+    out, segs = ot.project(starts, ends, mode, segments=True)
+    return pc, lp, out, segs
+
+
+def adjoint(pc, starts, ends, mode, out, gout, kernel_fields=None):
+    nf = pc._nfields
+    grad = np.zeros((len(pc.orig_ids), nf))
+    L.check(pc._cloud._lib.vt_project_adjoint(pc._cloud._h, L.dptr(np.ascontiguousarray(starts)),
+                                              L.dptr(np.ascontiguousarray(ends)), len(starts),
+                                              mode, L.dptr(np.ascontiguousarray(out)),
+                                              L.dptr(np.ascontiguousarray(gout)),
+                                              L.dptr(grad)))
+    return grad
+
+
+def sparse_sum_gradient(segs, nrays, npart, gout):
+    cid, se, sx, off = segs
+    ray = np.repeat(np.arange(nrays), np.diff(off))
+    A = sp.csr_matrix((sx - se, (ray, cid)), shape=(nrays, npart))
+    A.sum_duplicates()
+    return A.T @ gout
+
+
+def volume_reference_gradient(segs, fields, nrays, gout):
+    cid, se, sx, off = segs
+    grad = np.zeros_like(fields)
+    for r in range(nrays):
+        c = cid[off[r]:off[r + 1]]
+        ds = (sx - se)[off[r]:off[r + 1]]
+        rgb, a = fields[c, :3], fields[c, 3]
+        o = 1.0 - np.exp(-a * ds)
+        T = np.concatenate([[1.0], np.cumprod(1.0 - o)[:-1]])
+        contrib = (T * o)[:, None] * rgb
+        suffix = np.cumsum(contrib[::-1], axis=0)[::-1] - contrib  # sum over later segments
+        g = gout[r]
+        np.add.at(grad, (c, slice(0, 3)), (T * o)[:, None] * g[None, :])
+        ga = ds * np.sum(g[None, :] * (T[:, None] * rgb * (1.0 - o)[:, None] - suffix), axis=1)
+        np.add.at(grad[:, 3], c, ga)
+    return grad
+
+
+def fd_column(pc, fields_int, starts, ends, red, wts, cell, comp, h):
+    """Central difference of L = sum(W * img) w.r.t. fields_int[cell, comp]."""
+    f = fields_int.copy()
+    vals = []
+    for sgn in (1.0, -1.0):
+        f[cell, comp] = fields_int[cell, comp] + sgn * h
+        L.check(pc._cloud._lib.vt_cloud_set_fields(pc._cloud._h, L.dptr(f)))
+        vals.append(np.sum(wts * pc.projection(starts, ends, reduction=red).reshape(wts.shape)))
+    L.check(pc._cloud._lib.vt_cloud_set_fields(pc._cloud._h, L.dptr(fields_int)))
+    return (vals[0] - vals[1]) / (2.0 * h)
+
+
+@pytest.fixture(scope="module")
+def sum_case():
+    pos, rho = W.clustered_cloud(200_000, 11, nf=1)
+    s, e = W.z_grid([44.0, 56.0], 48)
+    return pos, rho, s, e
+
+
+def test_sum_adjoint_matches_sparse_reference(sum_case):
+    pos, rho, s, e = sum_case
+    pc, lp, out, segs = setup(pos, rho, W.BOX, s, e, "integrate")
+    g = np.random.default_rng(0).normal(size=(len(s), 1))
+    grad = adjoint(pc, s, e, L.REDUCE_SUM, out, g)
+    ref = sparse_sum_gradient(segs, len(s), len(lp["orig_ids"]), g)
+    np.testing.assert_allclose(grad, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())
+
+
+def test_sum_adjoint_multifield_and_hand_over(sum_case):
+    pos, rho, s, e = sum_case
+    f3 = np.column_stack([rho, 2 * rho, rho ** 2])
+    pc, lp, out, segs = setup(pos, f3, W.BOX, s, e, "integrate")
+    g = np.random.default_rng(1).normal(size=(len(s), 3))
+    ref = sparse_sum_gradient(segs, len(s), len(lp["orig_ids"]), g)
+    a = adjoint(pc, s, e, L.REDUCE_SUM, out, g)
+    np.testing.assert_allclose(a, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())
+    # every ray deeper than one pending point goes through the global-stack
+    # kernel, which must skip the segments already scattered
+    pc._cloud.set_param(L.PARAM_LOCAL_STACK, 1)
+    b = adjoint(pc, s, e, L.REDUCE_SUM, out, g)
+    pc._cloud.set_param(L.PARAM_LOCAL_STACK, 1 << 30)
+    np.testing.assert_allclose(b, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())
+
+
+def test_sum_adjoint_finite_differences(sum_case):
+    pos, rho, s, e = sum_case
+    pc, lp, out, segs = setup(pos, rho, W.BOX, s, e, "integrate")
+    wts = np.random.default_rng(2).normal(size=len(s))
+    grad = adjoint(pc, s, e, L.REDUCE_SUM, out, wts[:, None])[:, 0]
+    fint = lp["fields"].copy()
+    hit = np.nonzero(grad)[0]
+    cells = np.random.default_rng(3).choice(hit, 16, replace=False)
+    for c in cells:
+        fd = fd_column(pc, fint, s, e, "integrate", wts, c, 0, 1e-3 * max(1.0, abs(fint[c, 0])))
+        np.testing.assert_allclose(fd, grad[c], rtol=FD_RTOL)
+
+
+@pytest.fixture(scope="module")
+def vol_case():
+    pos, f = W.clustered_cloud(100_000, 12, nf=3)
+    rgba = W.transfer_rgba(f[:, 0] * 30.0)
+    s, e = W.z_grid([45.0, 55.0], 32)
+    return pos, rgba, s, e
+
+
+def test_volume_adjoint_matches_reference(vol_case):
+    pos, rgba, s, e = vol_case
+    pc, lp, out, segs = setup(pos, rgba, W.BOX, s, e, "volume")
+    g = np.random.default_rng(4).normal(size=(len(s), 3))
+    grad = adjoint(pc, s, e, L.REDUCE_VOLUME, out, g)
+    ref = volume_reference_gradient(segs, lp["fields"], len(s), g)
+    scale = np.abs(ref).max(axis=0)
+    np.testing.assert_allclose(grad, ref, rtol=1e-9, atol=1e-12 * scale.max())
+
+
+def test_volume_adjoint_finite_differences(vol_case):
+    pos, rgba, s, e = vol_case
+    pc, lp, out, segs = setup(pos, rgba, W.BOX, s, e, "volume")
+    wts = np.random.default_rng(5).normal(size=(len(s), 3))
+    grad = adjoint(pc, s, e, L.REDUCE_VOLUME, out, wts)
+    fint = lp["fields"].copy()
+    rng = np.random.default_rng(6)
+    inner = np.all((fint[:, :3] > 0.01) & (fint[:, :3] < 0.99), axis=1)
+    hit = np.nonzero((np.abs(grad).sum(1) > 0) & inner)[0]
+    checked = 0
+    for c in rng.choice(hit, min(64, len(hit)), replace=False):
+        comp = int(rng.integers(0, 4))
+        h = 1e-6 * max(1.0, abs(fint[c, comp]))
+        fd = fd_column(pc, fint, s, e, "volume", wts, c, comp, h)
+        if abs(grad[c, comp]) < 1e-8 * np.abs(grad).max():
+            continue  # below FD resolution
+        np.testing.assert_allclose(fd, grad[c, comp], rtol=FD_RTOL)
+        checked += 1
+    assert checked >= 16
+
+
+def test_autograd_function(sum_case, vol_case):
+    import torch
+    from vortrace_b200 import autograd as VA
+    pos, rho, s, e = sum_case
+    pc, lp, out, segs = setup(pos, rho, W.BOX, s, e, "integrate")
+    f = torch.tensor(rho, dtype=torch.float64, device="cuda", requires_grad=True)
+    img = VA.project(pc, f, s, e)
+    np.testing.assert_array_equal(img.detach().cpu().numpy(), out[:, 0])
+    wts = torch.randn(len(s), dtype=torch.float64, device="cuda")
+    (img * wts).sum().backward()
+    ref = sparse_sum_gradient(segs, len(s), len(lp["orig_ids"]), wts.cpu().numpy()[:, None])
+    want = np.zeros(len(rho))
+    want[lp["orig_ids"]] = ref[:, 0]
+    np.testing.assert_allclose(f.grad.cpu().numpy(), want, rtol=1e-12,
+                               atol=1e-14 * np.abs(want).max())
+    pos, rgba, s, e = vol_case
+    pc, lp, out, segs = setup(pos, rgba, W.BOX, s, e, "volume")
+    fv = torch.tensor(rgba, dtype=torch.float64, device="cuda", requires_grad=True)
+    imgv = VA.project(pc, fv, s, e, reduction="volume")
+    np.testing.assert_allclose(imgv.detach().cpu().numpy(), out, rtol=1e-12, atol=1e-300)
+    wv = torch.randn(len(s), 3, dtype=torch.float64, device="cuda")
+    (imgv * wv).sum().backward()
+    ref = volume_reference_gradient(segs, lp["fields"], len(s), wv.cpu().numpy())
+    want = np.zeros_like(rgba)
+    want[lp["orig_ids"]] = ref
+    np.testing.assert_allclose(fv.grad.cpu().numpy(), want, rtol=1e-9,
+                               atol=1e-12 * np.abs(want).max())

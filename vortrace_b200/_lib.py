@@ -30,12 +30,14 @@ PARAM_BLOCK_SIZE = 3
 PARAM_SMEM_LEVELS = 4
 PARAM_BLOCKS_PER_SM = 5
 PARAM_LEAF_SIZE = 6
+PARAM_LOCAL_STACK = 7
 
 # every symbol the header declares (checked by the tests)
 EXPORTS = (
     "vt_abi_version", "vt_last_error", "vt_set_verbose", "vt_get_verbose",
     "vt_set_warning_callback", "vt_set_device", "vt_cloud_create", "vt_cloud_build_tree",
-    "vt_cloud_set_param", "vt_cloud_get_info", "vt_cloud_orig_ids", "vt_cloud_destroy", "vt_knn",
+    "vt_cloud_set_param", "vt_cloud_set_fields", "vt_cloud_set_fields_device",
+    "vt_cloud_get_info", "vt_cloud_orig_ids", "vt_cloud_destroy", "vt_knn",
     "vt_project", "vt_project_device", "vt_project_detailed", "vt_segments_count",
     "vt_segments_copy", "vt_segments_free", "vt_project_adjoint", "vt_project_adjoint_device",
 )
@@ -98,6 +100,8 @@ def load(path: str | None = None):
                                       C.POINTER(vp)]
         L.vt_cloud_build_tree.argtypes = [vp]
         L.vt_cloud_set_param.argtypes = [vp, C.c_int, C.c_int64]
+        L.vt_cloud_set_fields.argtypes = [vp, dp]
+        L.vt_cloud_set_fields_device.argtypes = [vp, vp, vp]
         L.vt_cloud_get_info.argtypes = [vp, C.POINTER(CloudInfo)]
         L.vt_cloud_orig_ids.argtypes = [vp, i64p, u64]
         L.vt_cloud_destroy.argtypes = [vp]
@@ -115,6 +119,7 @@ def load(path: str | None = None):
         L.vt_project_adjoint.argtypes = [vp, dp, dp, u64, C.c_int, dp, dp, dp]
         L.vt_project_adjoint_device.argtypes = [vp, vp, vp, u64, C.c_int, vp, vp, vp, vp]
         for name in ("vt_cloud_create", "vt_cloud_build_tree", "vt_cloud_set_param",
+                     "vt_cloud_set_fields", "vt_cloud_set_fields_device",
                      "vt_cloud_get_info", "vt_cloud_orig_ids", "vt_knn", "vt_project",
                      "vt_project_device", "vt_project_detailed", "vt_segments_copy",
                      "vt_project_adjoint", "vt_project_adjoint_device", "vt_set_device"):

@@ -296,6 +296,10 @@ int vt_cloud_set_param(vt_cloud* cl, int param, int64_t value) {
       if (value < 0 || value > 64) return set_error(VT_ERR_INVALID, "blocks per SM out of range");
       cl->blocks_per_sm = (int)value;
       return VT_OK;
+    case VT_PARAM_LOCAL_STACK:
+      if (value < 1) return set_error(VT_ERR_INVALID, "local stack size must be >= 1");
+      cl->local_stack = value > (1 << 30) ? (1 << 30) : (int)value;
+      return VT_OK;
     case VT_PARAM_LEAF_SIZE:
       if (value < 2 || value > 64) return set_error(VT_ERR_INVALID, "leaf size out of range [2, 64]");
       cl->leaf_size = (int)value;
@@ -303,6 +307,29 @@ int vt_cloud_set_param(vt_cloud* cl, int param, int64_t value) {
     default:
       return set_error(VT_ERR_INVALID, "unknown parameter " + std::to_string(param));
   }
+}
+
+int vt_cloud_set_fields(vt_cloud* cl, const double* fields) {
+  VT_GUARD_BEGIN
+  if (!cl || !fields) return set_error(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  if (!cl->tree_built)
+    return set_error(VT_ERR_RUNTIME, "There is currently no valid tree for this point cloud");
+  VT_CUDA(cudaSetDevice(cl->device));
+  memcpy(cl->fields.data(), fields, cl->npart * cl->nfields * sizeof(double));
+  return vt::upload_fields(cl, fields, false, cl->stream);
+  VT_GUARD_END
+}
+
+int vt_cloud_set_fields_device(vt_cloud* cl, const double* d_fields, void* stream) {
+  VT_GUARD_BEGIN
+  if (!cl || !d_fields) return set_error(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  if (!cl->tree_built)
+    return set_error(VT_ERR_RUNTIME, "There is currently no valid tree for this point cloud");
+  VT_CUDA(cudaSetDevice(cl->device));
+  return vt::upload_fields(cl, d_fields, true, pick_stream(cl, stream));
+  VT_GUARD_END
 }
 
 int vt_cloud_get_info(const vt_cloud* cl, vt_cloud_info* info) {

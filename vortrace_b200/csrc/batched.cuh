@@ -281,6 +281,7 @@ __global__ void __launch_bounds__(128) k_batched(DevCloud c, WalkIO io, int nsm)
   double cur_s = 0.0, entry_s = 0.0, nxt_s = 0.0, s_split = 0.0;
   int64_t iter = 0;
   LocalStack<kBatchStack> st;
+  st.set_cap(io.local_cap);
   st.clear();
   double q_err = 0.0;
   // sinks
@@ -426,7 +427,9 @@ __global__ void __launch_bounds__(128) k_batched(DevCloud c, WalkIO io, int nsm)
     }
 
     // ---- apply
-    if (qkind == 1 && phase == 1) {
+    if (qkind != 0 && r.id[0] < 0) {
+      fail(kErrNonFiniteDist);  // squared distances overflowed
+    } else if (qkind == 1 && phase == 1) {
       c0 = r.id[0];
       phase = 2;
     } else if (qkind == 1 && phase == 2) {

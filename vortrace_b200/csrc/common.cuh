@@ -37,6 +37,7 @@ constexpr int kErrBinSearch = 12;
 constexpr int kErrPerturb = 13;
 constexpr int kErrKnnExpand = 14;
 constexpr int kErrStack = 15;
+constexpr int kErrNonFiniteDist = 17;  // squared distances overflowed
 // internal: the ray must be finished by the degenerate-geometry kernel
 constexpr int kNeedSlow = 99;
 

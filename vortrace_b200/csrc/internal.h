@@ -103,6 +103,7 @@ struct vt_cloud {
   int block_size = 128;
   int smem_levels = 9;
   int blocks_per_sm = 0;
+  int local_stack = 1 << 30;  // capped to the compiled size in the kernels
   // device tree (tree order)
   vt::DevBuf<double4> pts_d;
   vt::DevBuf<float4> pts32_d;
@@ -124,4 +125,5 @@ struct vt_cloud {
 
 namespace vt {
 int build_tree_device(vt_cloud* cl);
+int upload_fields(vt_cloud* cl, const double* src, bool src_device, cudaStream_t st);
 }

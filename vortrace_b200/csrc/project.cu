@@ -251,6 +251,7 @@ __global__ void __launch_bounds__(128) k_plain(DevCloud c, WalkIO io) {
   if (ray >= io.nrays) return;
   Search64 S(c);
   LocalStack<kPlainStack> st;
+  st.set_cap(io.local_cap);
   st.clear();
   unsigned nseg = 0;
   int rc = run_ray<MODE, NF, OUT>(c, io, ray, S, st, 0u, nseg);
@@ -297,9 +298,13 @@ __global__ void k_diag(DevCloud c, WalkIO io, int64_t ray) {
   st.cap = io.gstack_cap;
   RayGeom g;
   ray_init(g, io.starts + 3 * ray, io.ends + 3 * ray);
+  io.diag->code = 0;
+  if (!ray_finite(g)) {
+    io.diag->code = kErrNonFinite;
+    return;
+  }
   Search64 S(c);
   NullSink ns;
-  io.diag->code = 0;
   int rc = walk_ray(c, g, io.max_iter, S, st, ns, io.diag);
   if (rc == kNeedSlow) rc = kErrStack;
   io.diag->code = rc;
@@ -398,6 +403,7 @@ int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaS
   io.gstack_cap = cl->stack_cap;
   io.slow_threads = slow_threads;
   io.max_iter = cl->max_iter;
+  io.local_cap = cl->local_stack;
   io.diag = nullptr;
   VT_CUDA(cudaMemsetAsync(io.stats, 0, sizeof(DevStats), st));
   VT_CUDA(cudaMemsetAsync(&io.stats->first_error, 0xff, sizeof(unsigned long long), st));
@@ -473,7 +479,12 @@ int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaS
         msg = "Ray walk exceeded the pending-point stack capacity (" +
               std::to_string(cl->stack_cap) + ")";
         break;
-      case kErrNonFinite: msg = "Ray endpoints must be finite"; return set_error(VT_ERR_INVALID, msg + " (ray " + std::to_string(ray) + ")");
+      case kErrNonFinite:
+        return set_error(VT_ERR_INVALID,
+                         "Ray endpoints must be finite (ray " + std::to_string(ray) + ")");
+      case kErrNonFiniteDist:
+        return set_error(VT_ERR_INVALID, "Squared distances overflow for ray " +
+                                             std::to_string(ray) + ": coordinates too large");
       default: msg = "ray walk failed with code " + std::to_string(code); break;
     }
     return set_error(code, msg);

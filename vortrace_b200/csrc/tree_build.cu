@@ -239,6 +239,50 @@ __global__ void k_fields_tree(const double* __restrict__ f_in, const int32_t* __
 
 static inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
+// valid_rgba over internal-order fields (src/pointcloud.cpp:167-179)
+__global__ void k_rgba_check(const double* __restrict__ f, int64_t n, int* bad) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double r = f[4 * i], g = f[4 * i + 1], b = f[4 * i + 2], a = f[4 * i + 3];
+  if (!(r >= 0.0 && r <= 1.0 && g >= 0.0 && g <= 1.0 && b >= 0.0 && b <= 1.0 && a >= 0.0))
+    atomicOr(bad, 1);
+}
+
+// Replace the tree-order field array from internal-order values.
+int upload_fields(vt_cloud* cl, const double* src, bool src_device, cudaStream_t st) {
+  const int64_t n = (int64_t)cl->npart;
+  const int nf = (int)cl->nfields;
+  const int B = 256;
+  DevBuf<double> fin;
+  const double* dsrc = src;
+  int rc;
+  if (!src_device) {
+    if ((rc = fin.alloc((size_t)n * nf))) return rc;
+    VT_CUDA(cudaMemcpyAsync(fin.p, src, (size_t)n * nf * sizeof(double), cudaMemcpyHostToDevice,
+                            st));
+    dsrc = fin.p;
+  }
+  k_fields_tree<<<nblk((int64_t)n * nf, B), B, 0, st>>>(dsrc, cl->perm_d.p, n, nf,
+                                                        cl->fields_d.p);
+  VT_CUDA(cudaGetLastError());
+  bool valid = false;
+  if (nf == 4 && n > 0) {
+    DevBuf<int> bad;
+    if ((rc = bad.alloc(1))) return rc;
+    VT_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
+    k_rgba_check<<<nblk(n, B), B, 0, st>>>(dsrc, n, bad.p);
+    VT_CUDA(cudaGetLastError());
+    int hb = 1;
+    VT_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    VT_CUDA(cudaStreamSynchronize(st));
+    valid = hb == 0;
+  } else {
+    VT_CUDA(cudaStreamSynchronize(st));
+  }
+  cl->valid_rgba = valid;
+  return VT_OK;
+}
+
 // Build the device tree of `cl` from its host points/fields.
 int build_tree_device(vt_cloud* cl) {
   const int64_t n = (int64_t)cl->npart;

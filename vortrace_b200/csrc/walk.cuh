@@ -75,8 +75,10 @@ struct LocalStack {
   int id[CAP];
   double s[CAP];
   int sp, maxsp;
+  int cap = CAP;  // usable entries (<= CAP)
+  __device__ __forceinline__ void set_cap(int c) { cap = c < CAP ? (c > 1 ? c : 1) : CAP; }
   __device__ __forceinline__ void clear() { sp = maxsp = 0; }
-  __device__ __forceinline__ bool full() const { return sp >= CAP; }
+  __device__ __forceinline__ bool full() const { return sp >= cap; }
   __device__ __forceinline__ bool empty() const { return sp == 0; }
   __device__ __forceinline__ void push(int i, double v) {
     id[sp] = i;
@@ -87,7 +89,7 @@ struct LocalStack {
   __device__ __forceinline__ void pop() { --sp; }
   __device__ __forceinline__ int top_id() const { return id[sp - 1]; }
   __device__ __forceinline__ double top_s() const { return s[sp - 1]; }
-  __device__ __forceinline__ int room() const { return CAP - sp; }
+  __device__ __forceinline__ int room() const { return cap - sp; }
 };
 
 struct GlobalStack {
@@ -154,6 +156,7 @@ __device__ int split_full(const DevCloud& c, const RayGeom& g, S& srch, int id1,
     double x, y, z;
     ray_point(g, mid, x, y, z);
     const int mc = srch.nn1(x, y, z);
+    if (mc < 0) return kErrNonFiniteDist;
     if (mc != id1 && mc != id2) {
       s_out = mid;
       return 0;
@@ -251,6 +254,7 @@ __device__ int walk_ray(const DevCloud& c, const RayGeom& g, int64_t max_iter, S
                         Stack& st, Sink& sink, WalkDiag* diag) {
   const int c0 = srch.nn1(g.s[0], g.s[1], g.s[2]);
   const int c1 = srch.nn1(g.e[0], g.e[1], g.e[2]);
+  if (c0 < 0 || c1 < 0) return kErrNonFiniteDist;  // squared distances overflowed
   int open_cell = c0;
   double entry_s = 0.0;
   if (c0 == c1) {
@@ -308,6 +312,7 @@ __device__ int walk_ray(const DevCloud& c, const RayGeom& g, int64_t max_iter, S
     KnnList<3> r;
     rc = srch.knn3(x, y, z, cur, nxt, r);
     if (rc) return rc;
+    if (r.id[0] < 0) return kErrNonFiniteDist;
     bool has_c = false, has_n = false, three_eq = true;
 #pragma unroll
     for (int i = 0; i < 3; i++) {

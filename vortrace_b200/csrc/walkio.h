@@ -37,6 +37,7 @@ struct WalkIO {
   int gstack_cap;
   int slow_threads;
   int64_t max_iter;
+  int local_cap;         // in-register stack entries per ray
   WalkDiag* diag;
 };
 
