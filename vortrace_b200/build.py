@@ -60,15 +60,21 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in _deps())
 
 
-def build(force: bool = False, ptxas_verbose: bool = False, jobs: int = 0) -> str:
-    if not force and up_to_date():
+def build(force: bool = False, ptxas_verbose: bool = False, jobs: int = 0,
+          out: str | None = None, defines: tuple = ()) -> str:
+    """Compile and link; ``out``/``defines`` build a variant elsewhere (for
+    tuning sweeps, e.g. defines=("VT_BATCHED_MINB=6",))."""
+    lib = out or LIB
+    if out is None and not defines and not force and up_to_date():
         return LIB
-    os.makedirs(BUILD, exist_ok=True)
+    bdir = BUILD if out is None else lib + ".objs"
+    os.makedirs(bdir, exist_ok=True)
     cc = nvcc()
     objs, procs = [], []
     for src in _sources():
-        obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
-        cmd = [cc, *ARCH, *FLAGS, *host_compiler(), "-c", src, "-o", obj]
+        obj = os.path.join(bdir, os.path.basename(src)[:-3] + ".o")
+        cmd = [cc, *ARCH, *FLAGS, *host_compiler(), *[f"-D{d}" for d in defines], "-c", src,
+               "-o", obj]
         if ptxas_verbose:
             cmd += ["-Xptxas", "-v"]
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
@@ -84,10 +90,10 @@ def build(force: bool = False, ptxas_verbose: bool = False, jobs: int = 0) -> st
             sys.stderr.write(out)
     if failed:
         raise RuntimeError("libvortrace_b200 build failed")
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     subprocess.run([cc, *ARCH, *host_compiler(), "-shared", *objs, "-o", tmp], check=True)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 def main():

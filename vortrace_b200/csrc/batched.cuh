@@ -27,6 +27,10 @@
 namespace vt {
 
 constexpr int kBatchStack = 32;
+// resident blocks per SM the batched kernel is compiled for (register cap)
+#ifndef VT_BATCHED_MINB
+#define VT_BATCHED_MINB 4
+#endif
 
 // ---- node fetch (shared memory for the top levels) ----------------------
 struct Fetch64 {
@@ -230,6 +234,157 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
   nverify += ver;
 }
 
+// Leaf-directed guarded FP32 bounded search.  The query ball B(q, sqrt(R))
+// always contains c (cid), so the search starts from c's leaf, whose index
+// is known without descending: leaf(c) = (((c+1) << depth) - 1) / n.  The
+// root-to-leaf path of that leaf is walked with independent node loads (no
+// data-dependent branching); every sibling subtree of the path whose box
+// (the conservative FP32 box implied by the path's splits) is within the
+// current threshold is pushed, the leaf is scanned, and the pushed
+// subtrees are then searched depth-first, deepest first.  Same acceptance
+// rule and FP64 re-check as knn3_guarded, so the result is the same exact
+// set; only the visiting order (and so the order of exactly tied points)
+// differs.
+template <class F>
+__device__ __forceinline__ void knn3_leafdir(const DevCloud& c, const F& fetch, double qx,
+                                             double qy, double qz, int cid, int nid, double dc,
+                                             double dn, double R, double G, KnnList<3>& res,
+                                             unsigned& nvisit, unsigned& nverify) {
+  const float q32[3] = {__double2float_rn(dsub(qx, c.origin[0])),
+                        __double2float_rn(dsub(qy, c.origin[1])),
+                        __double2float_rn(dsub(qz, c.origin[2]))};
+  res.clear();
+  double thr64 = R;
+  float thr32 = __double2float_ru(dadd(thr64, G));
+  const int D = c.depth;
+  const int64_t ninternal = c.nleaves - 1;
+  const int64_t leaf0 = ((((int64_t)cid + 1) << D) - 1) / c.n;
+  const int64_t h1 = ninternal + leaf0 + 1;  // 1-based heap index of the leaf
+  float Lb[3] = {c.bblo32[0], c.bblo32[1], c.bblo32[2]};
+  float Ub[3] = {c.bbhi32[0], c.bbhi32[1], c.bbhi32[2]};
+  int sp = 0;
+  int s_node[kMaxDepth + 2];
+  float s_off[kMaxDepth + 2][3];
+  float s_mind[kMaxDepth + 2];
+  unsigned visits = 0, ver = 0;
+  auto box_off = [](float q, float lo, float hi) -> float {
+    return q < lo ? __fsub_rn(lo, q) : (q > hi ? __fsub_rn(q, hi) : 0.f);
+  };
+  // --- the path: ancestors of the leaf, siblings within reach are pushed
+  for (int k = 0; k < D; ++k) {
+    const int a = (int)((h1 >> (D - k)) - 1);
+    const int right = (int)((h1 >> (D - k - 1)) & 1);
+    const float2 nd = fetch(a);
+    const int dim = node_dim32(nd.x);
+    float sL = Lb[dim], sU = Ub[dim];
+    if (right) {  // path -> right child (p >= hi32); sibling = left (p <= lo32)
+      sU = fminf(sU, nd.x);
+      Lb[dim] = fmaxf(Lb[dim], nd.y);
+    } else {
+      sL = fmaxf(sL, nd.y);
+      Ub[dim] = fminf(Ub[dim], nd.x);
+    }
+    // sibling box = ancestor box with [sL, sU] along `dim` (Lb/Ub of the
+    // other dims are the ancestor's: only `dim` changed at this level)
+    float o[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float ob = box_off(q32[j], j == dim ? sL : Lb[j], j == dim ? sU : Ub[j]);
+      o[j] = __fmul_rn(ob, ob);
+    }
+    const float nm = __fadd_rn(__fadd_rn(o[0], o[1]), o[2]);
+    ++visits;
+    if (nm < thr32) {
+      s_node[sp] = right ? 2 * a + 1 : 2 * a + 2;
+      s_mind[sp] = nm;
+      s_off[sp][0] = o[0];
+      s_off[sp][1] = o[1];
+      s_off[sp][2] = o[2];
+      ++sp;
+    }
+  }
+  // --- scan c's leaf, then the pushed subtrees
+  int64_t node = ninternal + leaf0;
+  float off[3] = {0.f, 0.f, 0.f};
+  for (;;) {
+    ++visits;
+    if (node < ninternal) {
+      const float2 nd = fetch(node);
+      const int dim = node_dim32(nd.x);
+      const float val = q32[dim];
+      const int first = 2 * (int)node + 1;
+      int best, other;
+      float o;
+      if (__fadd_rn(__fsub_rn(val, nd.x), __fsub_rn(val, nd.y)) < 0.f) {
+        best = first;
+        other = first + 1;
+        o = nd.y > val ? __fsub_rn(nd.y, val) : 0.f;
+      } else {
+        best = first + 1;
+        other = first;
+        o = val > nd.x ? __fsub_rn(val, nd.x) : 0.f;
+      }
+      const float t = __fmul_rn(o, o);
+      const float o0 = dim == 0 ? fmaxf(t, off[0]) : off[0];
+      const float o1 = dim == 1 ? fmaxf(t, off[1]) : off[1];
+      const float o2 = dim == 2 ? fmaxf(t, off[2]) : off[2];
+      const float nm = __fadd_rn(__fadd_rn(o0, o1), o2);
+      if (nm < thr32) {
+        s_node[sp] = other;
+        s_mind[sp] = nm;
+        s_off[sp][0] = o0;
+        s_off[sp][1] = o1;
+        s_off[sp][2] = o2;
+        ++sp;
+      }
+      node = best;
+      continue;
+    }
+    {
+      int64_t a, b;
+      leaf_range(c, node - ninternal, a, b);
+#pragma unroll 2
+      for (int64_t p = a; p < b; ++p) {
+        const float4 P = __ldg(&c.pts32[p]);
+        const float d0 = __fsub_rn(q32[0], P.x), d1 = __fsub_rn(q32[1], P.y),
+                    d2 = __fsub_rn(q32[2], P.z);
+        const float f =
+            __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
+        if (f < thr32) {
+          const int pi = (int)p;
+          double d;
+          if (pi == cid) d = dc;
+          else if (pi == nid) d = dn;
+          else {
+            d = metric(qx, qy, qz, ldg_pt(&c.pts[p]));
+            ++ver;
+          }
+          if (d < thr64) {
+            res.insert(d, pi);
+            thr64 = fmin(R, res.worst());
+            thr32 = __double2float_ru(dadd(thr64, G));
+          }
+        }
+      }
+    }
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      if (s_mind[sp] < thr32) {
+        node = s_node[sp];
+        off[0] = s_off[sp][0];
+        off[1] = s_off[sp][1];
+        off[2] = s_off[sp][2];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  nvisit += visits;
+  nverify += ver;
+}
+
 // A bounded result B (all points with d < R, at most 3, exact order) gives
 // the same walk decisions as the unbounded 3-NN T when:
 //   * |B| == 3 (then B == T), or
@@ -252,9 +407,61 @@ __device__ __forceinline__ double guard_band(double R, double e) {
   return 1.02 * (6.0 * u * (R + cross) + cross + 1e-15 * R);
 }
 
+// ------------------------------------------------- rare paths, not inlined
+struct RareOut {
+  double s;
+  int rc, a, b;
+  unsigned nq;
+};
+
+// Parallel-bisector fallback of the split point (src/ray.cpp:96-126).
+__device__ __noinline__ RareOut rare_split(const DevCloud& c, RayGeom g, int cur, int nxt,
+                                           double cur_s, double nxt_s) {
+  Search64 S(c);
+  RareOut o{0.0, 0, 0, 0, 0u};
+  o.rc = split_full(c, g, S, cur, nxt, cur_s, nxt_s, o.s);
+  o.nq = S.nq;
+  return o;
+}
+
+// Case 1a (src/ray.cpp:364-422): intermediate cells on both sides.
+__device__ __noinline__ RareOut rare_case1a(const DevCloud& c, RayGeom g, double x, double y,
+                                            double z, int cur, int nxt) {
+  Search64 S(c);
+  int sc = try_along_ray(g, S, x, y, z, -1.0, cur, nxt);
+  if (sc < 0) {
+    const double ex = dmul(kPerturbEps, g.d[0]), ey = dmul(kPerturbEps, g.d[1]),
+                 ez = dmul(kPerturbEps, g.d[2]);
+    sc = perp_perturb(g, S, dsub(x, ex), dsub(y, ey), dsub(z, ez), cur, nxt);
+  }
+  int sn = -1;
+  if (sc >= 0) {
+    sn = try_along_ray(g, S, x, y, z, 1.0, cur, nxt);
+    if (sn < 0) {
+      const double ex = dmul(kPerturbEps, g.d[0]), ey = dmul(kPerturbEps, g.d[1]),
+                   ez = dmul(kPerturbEps, g.d[2]);
+      sn = perp_perturb(g, S, dadd(x, ex), dadd(y, ey), dadd(z, ez), cur, nxt);
+    }
+  }
+  RareOut o{0.0, (sc < 0 || sn < 0) ? kErrPerturb : 0, sc, sn, S.nq};
+  return o;
+}
+
+// 100-NN classification (src/ray.cpp:319-338).
+__device__ __noinline__ RareOut rare_expand(const DevCloud& c, double x, double y, double z,
+                                            int cur, int nxt) {
+  bool has_c = false, has_n = false;
+  unsigned v = 0;
+  RareOut o{0.0, 0, 0, 0, 1u};
+  o.rc = expand_classify(c, x, y, z, cur, nxt, has_c, has_n, v);
+  o.a = has_c;
+  o.b = has_n;
+  return o;
+}
+
 // --------------------------------------------------------------- kernel
 template <int MODE, int NF, int OUT, bool G32>
-__global__ void __launch_bounds__(128) k_batched(DevCloud c, WalkIO io, int nsm) {
+__global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, WalkIO io, int nsm) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // stage the top tree levels
   if (G32) {
@@ -387,8 +594,18 @@ __global__ void __launch_bounds__(128) k_batched(DevCloud c, WalkIO io, int nsm)
         const double4 pn = ldg_pt(&c.pts[nxt]);
         double s = split_analytic(g, pc, pn);
         if (!(s < DBL_MAX * 0.5 && s >= cur_s - kTol && s <= nxt_s + kTol)) {
-          fail(kNeedSlow);  // parallel-bisector bisection search
-          break;
+          // parallel bisector: bisection with nearest-neighbour queries
+          const RareOut ro = rare_split(c, g, cur, nxt, cur_s, nxt_s);
+          n_q += ro.nq;
+          s = ro.s;
+          if (ro.rc) {
+            fail(ro.rc);
+            break;
+          }
+          if (s < dsub(cur_s, kTol) || s > dadd(nxt_s, kTol)) {
+            fail(kErrSplitBounds);
+            break;
+          }
         }
         {
           const double lo = dadd(cur_s, 1e-15), hi = dsub(nxt_s, 1e-15);
@@ -414,7 +631,7 @@ __global__ void __launch_bounds__(128) k_batched(DevCloud c, WalkIO io, int nsm)
       ++n_q;
       if (G32) {
         const double G = guard_band(R, q_err);
-        knn3_guarded(c, f32, qx, qy, qz, cur, nxt, dc, dn, R, G, r, n_visit, n_ver);
+        knn3_leafdir(c, f32, qx, qy, qz, cur, nxt, dc, dn, R, G, r, n_visit, n_ver);
       } else {
         r.clear();
         knn64_fetch(c, f64, qx, qy, qz, R, r, n_visit);
@@ -458,8 +675,18 @@ __global__ void __launch_bounds__(128) k_batched(DevCloud c, WalkIO io, int nsm)
         if (r.id[i] == cur) has_c = true;
         if (r.id[i] == nxt) has_n = true;
       }
+      bool expand_failed = false;
       if (three_eq && !has_c && !has_n) {
-        fail(kNeedSlow);  // 100-NN expansion
+        const RareOut ro = rare_expand(c, qx, qy, qz, cur, nxt);
+        n_q += ro.nq;
+        if (ro.rc) {
+          fail(ro.rc);
+          expand_failed = true;
+        }
+        has_c = ro.a;
+        has_n = ro.b;
+      }
+      if (expand_failed) {
       } else if (has_c || has_n) {
         emit(open_cell, entry_s, s_split);
         open_cell = nxt;
@@ -475,7 +702,19 @@ __global__ void __launch_bounds__(128) k_batched(DevCloud c, WalkIO io, int nsm)
         if (st.room() < 1) fail(kNeedSlow);
         else st.push(r.id[0], s_split);
       } else {
-        fail(kNeedSlow);  // Case 1a
+        const RareOut ro = rare_case1a(c, g, qx, qy, qz, cur, nxt);
+        n_q += ro.nq;
+        const int sc = ro.a, sn = ro.b;
+        if (ro.rc) fail(ro.rc);
+        else if (sc == sn) {
+          if (st.room() < 1) fail(kNeedSlow);
+          else st.push(sc, s_split);
+        } else if (st.room() < 2) {
+          fail(kNeedSlow);
+        } else {
+          st.push(sn, s_split);
+          st.push(sc, s_split);
+        }
       }
     }
   }

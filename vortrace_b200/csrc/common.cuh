@@ -56,6 +56,7 @@ struct DevCloud {
   int depth;
   double bblo[3], bbhi[3];  // tight box of all points (nanoflann root_bbox)
   double origin[3];         // frame of pts32 / nodes32
+  float bblo32[3], bbhi32[3];  // root box in that frame, rounded outward
   float coord_err;          // bound on |pts32 - (p - origin)| per component
 };
 

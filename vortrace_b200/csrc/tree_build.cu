@@ -25,6 +25,7 @@
 //      node copy rounded outward.
 #include <cub/cub.cuh>
 
+#include <cmath>
 #include <cstdio>
 #include <vector>
 
@@ -435,6 +436,11 @@ int build_tree_device(vt_cloud* cl) {
     v.bblo[j] = lo[j];
     v.bbhi[j] = hi[j];
     v.origin[j] = org[j];
+    // outward-rounded FP32 root box (all pts32 lie inside it)
+    v.bblo32[j] = std::nextafter((float)(lo[j] - org[j]), -INFINITY);
+    v.bbhi32[j] = std::nextafter((float)(hi[j] - org[j]), INFINITY);
+    v.bblo32[j] = std::nextafter(v.bblo32[j], -INFINITY);
+    v.bbhi32[j] = std::nextafter(v.bbhi32[j], INFINITY);
   }
   // |fl32(p - o) - (p - o)| <= 2^-24 |p - o| (plus the FP64 subtraction)
   v.coord_err = (float)(mext * 6.0e-8 + 1e-300);
