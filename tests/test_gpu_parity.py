@@ -16,7 +16,7 @@ from vortrace_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = ["plain", "batched", "batched_fp64"]
+KERNELS = ["plain", "batched", "batched_fp64", "thread_fp32"]
 VOL_RTOL = 1e-12
 
 

@@ -21,8 +21,9 @@ VT_ERR_NOMEM = 4
 
 REDUCE_SUM, REDUCE_MAX, REDUCE_MIN, REDUCE_VOLUME = 0, 1, 2, 3
 KERNEL_AUTO, KERNEL_PLAIN_FP64, KERNEL_BATCHED, KERNEL_BATCHED_FP64 = 0, 1, 2, 3
+KERNEL_THREAD_FP32 = 4
 KERNELS = {"auto": KERNEL_AUTO, "plain": KERNEL_PLAIN_FP64, "batched": KERNEL_BATCHED,
-           "batched_fp64": KERNEL_BATCHED_FP64}
+           "batched_fp64": KERNEL_BATCHED_FP64, "thread_fp32": KERNEL_THREAD_FP32}
 
 PARAM_MAX_ITERATIONS = 1
 PARAM_STACK_CAP = 2

@@ -345,7 +345,8 @@ int vt_cloud_get_info(const vt_cloud* cl, vt_cloud_info* info) {
   info->tree_leaves = cl->tree_built ? (uint64_t)cl->view.nleaves : 0;
   info->tree_build_ms = cl->build_ms;
   info->device_bytes = cl->pts_d.bytes() + cl->pts32_d.bytes() + cl->nodes_d.bytes() +
-                       cl->nodes32_d.bytes() + cl->perm_d.bytes() + cl->fields_d.bytes();
+                       cl->nodes32_d.bytes() + cl->perm_d.bytes() + cl->fields_d.bytes() +
+                       cl->boxlo_d.bytes() + cl->boxhi_d.bytes();
   return VT_OK;
 }
 

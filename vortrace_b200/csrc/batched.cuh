@@ -727,7 +727,7 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
 
 template <int MODE, int NF, int OUT>
 int launch_batched(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) {
-  const bool g32 = kernel != VT_KERNEL_BATCHED_FP64;
+  const bool g32 = kernel == VT_KERNEL_THREAD_FP32;
   const int64_t ninternal = cl->view.nleaves - 1;
   int64_t want = (1LL << cl->smem_levels) - 1;
   int nsm = (int)(want < ninternal ? want : ninternal);

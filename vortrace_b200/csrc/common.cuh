@@ -50,6 +50,10 @@ struct DevCloud {
   const float2* __restrict__ nodes32;
   const int32_t* __restrict__ perm;
   const double* __restrict__ fields;
+  // tight FP32 boxes (of the pts32 values) of every heap node, internal
+  // nodes first then leaves: node i in [0, 2L-1)
+  const float4* __restrict__ boxlo;
+  const float4* __restrict__ boxhi;
   int64_t n;
   int64_t nleaves;  // 2^depth
   int nf;

@@ -111,6 +111,7 @@ struct vt_cloud {
   vt::DevBuf<float2> nodes32_d;
   vt::DevBuf<int32_t> perm_d;
   vt::DevBuf<double> fields_d;
+  vt::DevBuf<float4> boxlo_d, boxhi_d;
   vt::DevCloud view{};
   double build_ms = 0.0;
   // per-call workspace (grow-only)

@@ -332,8 +332,10 @@ __global__ void k_knn(DevCloud c, const double* __restrict__ q, int64_t nq, int 
 
 }  // namespace vt
 
-// batched kernel (persistent, guarded FP32)
+// persistent kernels: one ray per thread (batched.cuh), one ray per warp
+// with warp-cooperative search (warp.cuh)
 #include "batched.cuh"
+#include "warp.cuh"
 
 namespace vt {
 
@@ -345,6 +347,9 @@ static int launch_walk_t(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) 
     if (kernel == VT_KERNEL_PLAIN_FP64) {
       const int B = 128;
       k_plain<MODE, NF, OUT><<<(unsigned)((io.nrays + B - 1) / B), B, 0, st>>>(c, io);
+    } else if (kernel == VT_KERNEL_BATCHED && cl->nfields <= 32) {
+      int rc = launch_warp<MODE, OUT>(cl, io, st);
+      if (rc) return rc;
     } else {
       int rc = launch_batched<MODE, NF, OUT>(cl, io, kernel, st);
       if (rc) return rc;

@@ -240,6 +240,33 @@ __global__ void k_fields_tree(const double* __restrict__ f_in, const int32_t* __
 
 static inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
+// Tight boxes of the FP32 point copies: leaves from their points ...
+__global__ void k_leaf_boxes(const float4* __restrict__ pts32, int64_t n, int depth,
+                             int64_t nleaves, float4* lo, float4* hi) {
+  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= nleaves) return;
+  const int64_t a = (j * n) >> depth, b = ((j + 1) * n) >> depth;
+  float4 l = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+  float4 h = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+  for (int64_t p = a; p < b; ++p) {
+    const float4 v = pts32[p];
+    l.x = fminf(l.x, v.x); l.y = fminf(l.y, v.y); l.z = fminf(l.z, v.z);
+    h.x = fmaxf(h.x, v.x); h.y = fmaxf(h.y, v.y); h.z = fmaxf(h.z, v.z);
+  }
+  lo[nleaves - 1 + j] = l;
+  hi[nleaves - 1 + j] = h;
+}
+
+// ... internal nodes of one level as the union of their children.
+__global__ void k_level_boxes(int lvl, float4* lo, float4* hi) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= (1LL << lvl)) return;
+  const int64_t i = (1LL << lvl) - 1 + k;
+  const float4 a = lo[2 * i + 1], b = lo[2 * i + 2], c = hi[2 * i + 1], d = hi[2 * i + 2];
+  lo[i] = make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), 0.f);
+  hi[i] = make_float4(fmaxf(c.x, d.x), fmaxf(c.y, d.y), fmaxf(c.z, d.z), 0.f);
+}
+
 // valid_rgba over internal-order fields (src/pointcloud.cpp:167-179)
 __global__ void k_rgba_check(const double* __restrict__ f, int64_t n, int* bad) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -401,6 +428,12 @@ int build_tree_device(vt_cloud* cl) {
   VT_TRY(fields.alloc((int64_t)n * nf));
   k_finalize<<<nblk(n, B), B, 0, st>>>(ax.p, ay.p, az.p, n, org[0], org[1], org[2], pts.p,
                                        pts32.p);
+  DevBuf<float4> blo, bhi;
+  VT_TRY(blo.alloc(2 * nleaves - 1));
+  VT_TRY(bhi.alloc(2 * nleaves - 1));
+  k_leaf_boxes<<<nblk(nleaves, B), B, 0, st>>>(pts32.p, n, depth, nleaves, blo.p, bhi.p);
+  for (int l = depth - 1; l >= 0; --l)
+    k_level_boxes<<<nblk(1LL << l, B), B, 0, st>>>(l, blo.p, bhi.p);
   {
     // fields: upload in internal order into the (now free) aos buffer, gather
     DevBuf<double> fin;
@@ -421,6 +454,8 @@ int build_tree_device(vt_cloud* cl) {
   cl->nodes_d = std::move(nodes);
   cl->nodes32_d = std::move(nodes32);
   cl->fields_d = std::move(fields);
+  cl->boxlo_d = std::move(blo);
+  cl->boxhi_d = std::move(bhi);
   DevCloud& v = cl->view;
   v.pts = cl->pts_d.p;
   v.pts32 = cl->pts32_d.p;
@@ -428,6 +463,8 @@ int build_tree_device(vt_cloud* cl) {
   v.nodes32 = cl->nodes32_d.p;
   v.perm = cl->perm_d.p;
   v.fields = cl->fields_d.p;
+  v.boxlo = cl->boxlo_d.p;
+  v.boxhi = cl->boxhi_d.p;
   v.n = n;
   v.nleaves = nleaves;
   v.nf = nf;

@@ -1,0 +1,631 @@
+// warp.cuh -- the batched walk kernel: one warp per ray, warp-cooperative
+// guarded-FP32 k-NN.
+//
+// The walk of src/ray.cpp:187-430 runs with warp-uniform control flow: every
+// lane holds the same ray state, and only the k-NN searches and the field
+// reductions spread work over the lanes.
+//   * Work queue: lane 0 of a warp takes the next ray from a global atomic
+//     counter; long and short rays, many projections and arbitrary rays share
+//     one persistent launch.
+//   * k-NN ("wide" traversal of the implicit binary tree): a step expands one
+//     node into its descendants 5 levels down (32 nodes, contiguous in heap
+//     order, one per lane).  Each lane loads its node's tight FP32 box with two
+//     coalesced 128-bit loads and tests it against the threshold; a ballot
+//     gives the survivors, the nearest continues and the rest go on a per-warp
+//     stack in shared memory.  Leaf groups are expanded into their points,
+//     spread over the lanes (warp prefix sum + per-lane binary search), tested
+//     in FP32, and the few points that pass are re-checked with their FP64
+//     distance in the reference's operation order and inserted in lane order.
+//   * Guarded FP32: a point passes if f < thr64 + G, where G bounds the
+//     FP32 error of f for every point with d < R; box distances use the same
+//     rounding steps as f on box corners that are themselves FP32 point
+//     values, so box pruning never drops a point that would pass.  The FP64
+//     list is exact; only the order of exactly tied points can differ from
+//     nanoflann's.
+//   * Split queries are bounded by R = max(d_c, d_n) + 4 TOL (see
+//     knn3_decision_valid); end-point queries start from the leaf found by
+//     descending the split planes, then search bounded by its best distance.
+//   * The pending-point stack of the walk also lives in shared memory (64
+//     entries per warp); a deeper stack hands the ray to k_slow.
+#pragma once
+
+namespace vt {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarpsPerBlock = 4;
+constexpr int kWSearchStack = 128;  // per-warp search stack entries
+constexpr int kWWalkStack = 64;     // per-warp pending ray points
+#ifndef VT_WARP_MINB
+#define VT_WARP_MINB 8
+#endif
+
+__device__ __forceinline__ float box_dist32(float q0, float q1, float q2, float4 lo, float4 hi) {
+  const float a = q0 < lo.x ? __fsub_rn(lo.x, q0) : (q0 > hi.x ? __fsub_rn(q0, hi.x) : 0.f);
+  const float b = q1 < lo.y ? __fsub_rn(lo.y, q1) : (q1 > hi.y ? __fsub_rn(q1, hi.y) : 0.f);
+  const float c = q2 < lo.z ? __fsub_rn(lo.z, q2) : (q2 > hi.z ? __fsub_rn(q2, hi.z) : 0.f);
+  return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
+}
+
+__device__ __forceinline__ float pt_dist32(float q0, float q1, float q2, float4 p) {
+  const float a = __fsub_rn(q0, p.x), b = __fsub_rn(q1, p.y), c = __fsub_rn(q2, p.z);
+  return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
+}
+
+__device__ __forceinline__ int depth_of(int v) { return 31 - __clz(v + 1); }
+
+struct WarpQuery {
+  double x, y, z;     // FP64 query
+  float q0, q1, q2;   // FP32 frame
+  double bound, G;    // accept d < bound; FP32 guard band
+  int cid, nid;       // cells with known distances (or -1)
+  double dc, dn;
+};
+
+// Test the points of the leaves in `mask` (group starting at heap node
+// `gfirst`) and insert the ones with d < current threshold into L.
+template <int K>
+__device__ __forceinline__ void warp_leaves(const DevCloud& c, const int lane,
+                                            const WarpQuery& Q, const unsigned mask,
+                                            const int64_t gfirst, KnnList<K>& L, double& thr64,
+                                            float& thr32, unsigned& nver) {
+  const int64_t ninternal = c.nleaves - 1;
+  int64_t a = 0;
+  int cnt = 0;
+  if ((mask >> lane) & 1u) {
+    const int64_t j = gfirst + lane - ninternal;
+    a = (j * c.n) >> c.depth;
+    cnt = (int)((((j + 1) * c.n) >> c.depth) - a);
+  }
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int total = __shfl_sync(kFull, incl, 31);
+  for (int base = 0; base < total; base += 32) {
+    const int kk = base + lane;
+    int lo = 0, hi = 31;
+#pragma unroll
+    for (int it = 0; it < 5; ++it) {
+      const int mid = (lo + hi) >> 1;
+      const int vm = __shfl_sync(kFull, incl, mid);
+      if (vm > kk) hi = mid;
+      else lo = mid + 1;
+    }
+    const long long ao = __shfl_sync(kFull, (long long)a, lo);
+    const int exo = __shfl_sync(kFull, incl - cnt, lo);
+    const int64_t p = ao + (kk - exo);
+    const bool act = kk < total;
+    float f = __int_as_float(0x7f800000);
+    if (act) f = pt_dist32(Q.q0, Q.q1, Q.q2, __ldg(&c.pts32[p]));
+    const bool cand = act && f < thr32;
+    unsigned cm = __ballot_sync(kFull, cand);
+    if (!cm) continue;
+    double d = 0.0;
+    if (cand) {
+      const int pi = (int)p;
+      if (pi == Q.cid) d = Q.dc;
+      else if (pi == Q.nid) d = Q.dn;
+      else {
+        d = metric(Q.x, Q.y, Q.z, ldg_pt(&c.pts[p]));
+        ++nver;
+      }
+    }
+    while (cm) {
+      const int j = __ffs(cm) - 1;
+      cm &= cm - 1;
+      const double dj = __shfl_sync(kFull, d, j);
+      const int pj = __shfl_sync(kFull, (int)p, j);
+      if (dj < thr64) {
+        L.insert(dj, pj);
+        thr64 = fmin(Q.bound, L.worst());
+        thr32 = __double2float_ru(dadd(thr64, Q.G));
+      }
+    }
+  }
+}
+
+// Warp-cooperative exact K-NN among points with d < Q.bound; L may hold
+// results already (then `skip_leaf`, the leaf they came from, is skipped).
+// Returns false if the per-warp stack overflowed (the result is then not
+// trustworthy and the caller re-resolves the query).
+template <int K>
+__device__ bool warp_knn(const DevCloud& c, const int lane, const WarpQuery& Q,
+                         const int64_t skip_leaf, KnnList<K>& L, int* s_node, float* s_mind,
+                         unsigned& nver, unsigned& nsteps) {
+  const int D = c.depth;
+  const int64_t ninternal = c.nleaves - 1;
+  double thr64 = fmin(Q.bound, L.worst());
+  float thr32 = __double2float_ru(dadd(thr64, Q.G));
+  int sp = 0;
+  bool overflow = false;
+  // group being tested: nodes [gfirst, gfirst + gm), leaves if gleaves
+  int64_t gfirst;
+  int gm;
+  bool gleaves;
+  if (D == 0) {
+    gfirst = 0;
+    gm = 1;
+    gleaves = true;
+  } else {
+    const int s = ((D - 1) % 5) + 1;  // so that every later step spans 5 levels
+    gfirst = (1LL << s) - 1;
+    gm = 1 << s;
+    gleaves = (s == D);
+  }
+  for (;;) {
+    ++nsteps;
+    const int64_t node = gfirst + lane;
+    float nm = __int_as_float(0x7f800000);
+    bool surv = false;
+    if (lane < gm) {
+      nm = box_dist32(Q.q0, Q.q1, Q.q2, __ldg(&c.boxlo[node]), __ldg(&c.boxhi[node]));
+      surv = nm < thr32 && !(gleaves && node - ninternal == skip_leaf);
+    }
+    const unsigned mask = __ballot_sync(kFull, surv);
+    bool next = false;
+    int v = 0;
+    if (gleaves) {
+      if (mask) warp_leaves<K>(c, lane, Q, mask, gfirst, L, thr64, thr32, nver);
+    } else if (mask) {
+      const unsigned key = surv ? __float_as_uint(nm) : 0xffffffffu;
+      const unsigned kmin = __reduce_min_sync(kFull, key);
+      const int w = __ffs(__ballot_sync(kFull, key == kmin)) - 1;
+      const unsigned rest = mask & ~(1u << w);
+      const int cnt = __popc(rest);
+      if (sp + cnt > kWSearchStack) {
+        overflow = true;
+      } else if ((rest >> lane) & 1u) {
+        const int e = sp + __popc(rest & ((1u << lane) - 1u));
+        s_node[e] = (int)node;
+        s_mind[e] = nm;
+      }
+      if (!overflow) sp += cnt;
+      __syncwarp();
+      v = (int)(gfirst + w);
+      next = true;
+    }
+    if (!next) {
+      while (sp > 0) {
+        --sp;
+        const float pm = s_mind[sp];
+        if (pm < thr32) {
+          v = s_node[sp];
+          next = true;
+          break;
+        }
+      }
+      __syncwarp();
+      if (!next) break;
+    }
+    const int k = depth_of(v);
+    const int s = min(5, D - k);
+    gfirst = ((int64_t)(v + 1) << s) - 1;
+    gm = 1 << s;
+    gleaves = (k + s == D);
+  }
+  return !overflow;
+}
+
+// Leaf reached by descending the split planes from the root (uniform loads).
+__device__ __forceinline__ int64_t warp_descend_leaf(const DevCloud& c, float q0, float q1,
+                                                     float q2) {
+  const int64_t ninternal = c.nleaves - 1;
+  int64_t v = 0;
+  while (v < ninternal) {
+    const float2 nd = __ldg(&c.nodes32[v]);
+    const int dim = node_dim32(nd.x);
+    const float val = dim == 0 ? q0 : (dim == 1 ? q1 : q2);
+    v = __fadd_rn(__fsub_rn(val, nd.x), __fsub_rn(val, nd.y)) < 0.f ? 2 * v + 1 : 2 * v + 2;
+  }
+  return v - ninternal;
+}
+
+// Unbounded K-NN: the leaf on the split-plane path first (all its points
+// are candidates), then a search bounded by the K-th best distance found.
+template <int K>
+__device__ bool warp_knn_unbounded(const DevCloud& c, const int lane, WarpQuery Q, double qe,
+                                   KnnList<K>& L, int* s_node, float* s_mind, unsigned& nver,
+                                   unsigned& nsteps) {
+  L.clear();
+  const int64_t leaf = warp_descend_leaf(c, Q.q0, Q.q1, Q.q2);
+  {
+    const int64_t a = (leaf * c.n) >> c.depth;
+    const int cnt = (int)((((leaf + 1) * c.n) >> c.depth) - a);
+    for (int base = 0; base < cnt; base += 32) {
+      const int kk = base + lane;
+      double d = 0.0;
+      if (kk < cnt) d = metric(Q.x, Q.y, Q.z, ldg_pt(&c.pts[a + kk]));
+      const int m = min(32, cnt - base);
+      for (int j = 0; j < m; ++j) {
+        const double dj = __shfl_sync(kFull, d, j);
+        if (dj < L.worst()) L.insert(dj, (int)(a + base + j));
+      }
+    }
+  }
+  Q.bound = __longlong_as_double(0x7ff0000000000000LL);
+  Q.cid = Q.nid = -1;
+  // the threshold never exceeds the K-th distance found in the leaf
+  Q.G = guard_band(L.worst(), qe);
+  return warp_knn<K>(c, lane, Q, leaf, L, s_node, s_mind, nver, nsteps);
+}
+
+// Guard band for unbounded queries: the FP32 error bound at the current
+// threshold is re-derived when the threshold is known (G grows with R).
+__device__ __forceinline__ void warp_query_setup(WarpQuery& Q, const DevCloud& c, double x,
+                                                 double y, double z) {
+  Q.x = x;
+  Q.y = y;
+  Q.z = z;
+  Q.q0 = __double2float_rn(dsub(x, c.origin[0]));
+  Q.q1 = __double2float_rn(dsub(y, c.origin[1]));
+  Q.q2 = __double2float_rn(dsub(z, c.origin[2]));
+}
+
+// ------------------------------------------------------------------ sinks
+// Lane-parallel reduction: lane f accumulates field f (f < nf <= 32) with
+// the reference's sequence of operations per field.
+template <int MODE>
+struct WarpReducer {
+  double acc, T;
+  unsigned nseg;
+  __device__ __forceinline__ void init() {
+    nseg = 0;
+    T = 1.0;
+    acc = MODE == kMax ? -pinf() : (MODE == kMin ? pinf() : 0.0);
+  }
+  __device__ __forceinline__ void seg(const DevCloud& c, int lane, int cell, double a, double b) {
+    ++nseg;
+    const double ds = dsub(b, a);
+    if (MODE == kVolume) {
+      const double* F = c.fields + (int64_t)cell * 4;
+      const double alpha = F[3];
+      const double opac = dsub(1.0, exp(dmul(-alpha, ds)));
+      if (lane < 3) acc = dadd(acc, dmul(dmul(T, F[lane]), opac));
+      T = dmul(T, dsub(1.0, opac));
+    } else if (lane < c.nf) {
+      const double v = c.fields[(int64_t)cell * c.nf + lane];
+      if (MODE == kSum) acc = dadd(acc, dmul(ds, v));
+      else if (MODE == kMax) acc = v > acc ? v : acc;
+      else acc = v < acc ? v : acc;
+    }
+  }
+};
+
+// Lane-parallel adjoint (see AdjSink): lane f scatters field f.
+template <int MODE>
+struct WarpAdj {
+  double g, C, P, T;
+  unsigned nseg, skip;
+  __device__ __forceinline__ void init(const WalkIO& io, int lane, int64_t ray, unsigned sk) {
+    nseg = 0;
+    skip = sk;
+    T = 1.0;
+    P = 0.0;
+    g = lane < io.nout ? io.gout[ray * io.nout + lane] : 0.0;
+    C = (MODE == kVolume && lane < 3) ? io.fwd[ray * 3 + lane] : 0.0;
+  }
+  __device__ __forceinline__ void seg(const DevCloud& c, const WalkIO& io, int lane, int cell,
+                                      double a, double b) {
+    const bool emit = nseg >= skip;
+    ++nseg;
+    const double ds = dsub(b, a);
+    const int64_t pid = c.perm[cell];
+    if (MODE == kVolume) {
+      const double* F = c.fields + (int64_t)cell * 4;
+      const double alpha = F[3];
+      const double e = exp(dmul(-alpha, ds));
+      const double o = dsub(1.0, e);
+      double term = 0.0;
+      if (lane < 3) {
+        const double Fk = F[lane];
+        P = dadd(P, dmul(dmul(T, Fk), o));
+        term = g * (T * Fk * e - (C - P));
+        if (emit) atomicAdd(&io.grad[pid * 4 + lane], g * T * o);
+      }
+      term += __shfl_down_sync(kFull, term, 1);
+      term += __shfl_down_sync(kFull, term, 2);
+      if (emit && lane == 0) atomicAdd(&io.grad[pid * 4 + 3], ds * term);
+      T = dmul(T, dsub(1.0, o));
+    } else if (emit && lane < c.nf) {
+      atomicAdd(&io.grad[pid * c.nf + lane], g * ds);
+    }
+  }
+};
+
+// --------------------------------------------------------------- kernel
+template <int MODE, int OUT>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevCloud c, WalkIO io) {
+  __shared__ int s_node_all[kWarpsPerBlock][kWSearchStack];
+  __shared__ float s_mind_all[kWarpsPerBlock][kWSearchStack];
+  __shared__ int w_id_all[kWarpsPerBlock][kWWalkStack];
+  __shared__ double w_s_all[kWarpsPerBlock][kWWalkStack];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  int* s_node = s_node_all[wib];
+  float* s_mind = s_mind_all[wib];
+  int* w_id = w_id_all[wib];
+  double* w_s = w_s_all[wib];
+  const double cerr = (double)c.coord_err;
+  unsigned n_rays = 0, n_cross = 0, n_q = 0, n_res = 0, n_ver = 0, n_steps = 0, max_sp = 0;
+
+  for (;;) {
+    long long ray = 0;
+    if (lane == 0) ray = (long long)atomicAdd(&io.stats->next_ray, 1ULL);
+    ray = __shfl_sync(kFull, ray, 0);
+    if (ray >= io.nrays) break;
+    RayGeom g;
+    ray_init(g, io.starts + 3 * ray, io.ends + 3 * ray);
+    if (!ray_finite(g)) {
+      if (lane == 0) report(io, ray, kErrNonFinite);
+      continue;
+    }
+    ++n_rays;
+    double qe = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      qe = fmax(qe, fmax(fabs(g.s[j] - c.origin[j]), fabs(g.e[j] - c.origin[j])));
+    qe = qe * 6.0e-8 + cerr;
+
+    WarpReducer<MODE> red;
+    WarpAdj<MODE> adj;
+    unsigned fill_n = 0;
+    int64_t fill_off = 0;
+    if (OUT == kOutImage || OUT == kOutCount) red.init();
+    else if (OUT == kOutFill) fill_off = io.offsets[ray];
+    else adj.init(io, lane, ray, 0u);
+    auto emit = [&](int cell, double a, double b) {
+      if (OUT == kOutImage || OUT == kOutCount) red.seg(c, lane, cell, a, b);
+      else if (OUT == kOutFill) {
+        if (lane == 0) {
+          io.seg_cell[fill_off + fill_n] = c.perm[cell];
+          io.seg_enter[fill_off + fill_n] = a;
+          io.seg_exit[fill_off + fill_n] = b;
+        }
+        ++fill_n;
+      } else adj.seg(c, io, lane, cell, a, b);
+    };
+    auto nseg_now = [&]() -> unsigned {
+      return (OUT == kOutImage || OUT == kOutCount) ? red.nseg : (OUT == kOutFill ? fill_n : adj.nseg);
+    };
+
+    // ---- end cells
+    WarpQuery Q;
+    Q.G = guard_band(1.0, qe);  // unbounded queries re-bound below
+    KnnList<1> r1;
+    int cend[2];
+    bool ok = true;
+    for (int e = 0; e < 2; ++e) {
+      const double* pt = e == 0 ? g.s : g.e;
+      warp_query_setup(Q, c, pt[0], pt[1], pt[2]);
+      // exact: the guard is re-derived from the leaf's best distance
+      r1.clear();
+      const int64_t leaf = warp_descend_leaf(c, Q.q0, Q.q1, Q.q2);
+      {
+        const int64_t a = (leaf * c.n) >> c.depth;
+        const int cnt = (int)((((leaf + 1) * c.n) >> c.depth) - a);
+        for (int base = 0; base < cnt; base += 32) {
+          const int kk = base + lane;
+          double d = 0.0;
+          if (kk < cnt) d = metric(Q.x, Q.y, Q.z, ldg_pt(&c.pts[a + kk]));
+          const int m = min(32, cnt - base);
+          for (int j = 0; j < m; ++j) {
+            const double dj = __shfl_sync(kFull, d, j);
+            if (dj < r1.worst()) r1.insert(dj, (int)(a + base + j));
+          }
+        }
+      }
+      Q.bound = pinf();
+      Q.G = guard_band(r1.worst(), qe);
+      Q.cid = Q.nid = -1;
+      ++n_q;
+      if (!warp_knn<1>(c, lane, Q, leaf, r1, s_node, s_mind, n_ver, n_steps)) {
+        // search stack overflow: exact thread-level search by lane 0
+        ++n_res;
+        int id = -1;
+        if (lane == 0) {
+          unsigned v = 0;
+          id = nn1_exact64(c, Q.x, Q.y, Q.z, v);
+        }
+        r1.id[0] = __shfl_sync(kFull, id, 0);
+      }
+      cend[e] = r1.id[0];
+      if (cend[e] < 0) ok = false;
+    }
+    if (!ok) {
+      if (lane == 0) report(io, ray, kErrNonFiniteDist);
+      continue;
+    }
+    int rc = 0;
+    int cur = cend[0], open_cell = cend[0];
+    double cur_s = 0.0, entry_s = 0.0;
+    if (cend[0] == cend[1]) {
+      emit(cend[0], 0.0, g.len);
+    } else {
+      int sp = 1;
+      if (lane == 0) {
+        w_id[0] = cend[1];
+        w_s[0] = g.len;
+      }
+      __syncwarp();
+      int64_t iter = 0;
+      for (;;) {
+        if (++iter > io.max_iter) {
+          rc = kErrMaxIter;
+          break;
+        }
+        const int nxt = w_id[sp - 1];
+        const double nxt_s = w_s[sp - 1];
+        if (dsub(nxt_s, cur_s) < 1e-14) {  // zero-width skip
+          --sp;
+          cur = nxt;
+          cur_s = nxt_s;
+          open_cell = cur;
+          if (sp == 0) break;
+          continue;
+        }
+        const double4 pc = ldg_pt(&c.pts[cur]);
+        const double4 pn = ldg_pt(&c.pts[nxt]);
+        double s = split_analytic(g, pc, pn);
+        if (!(s < DBL_MAX * 0.5 && s >= cur_s - kTol && s <= nxt_s + kTol)) {
+          RareOut ro{0.0, 0, 0, 0, 0u};
+          if (lane == 0) ro = rare_split(c, g, cur, nxt, cur_s, nxt_s);
+          s = __shfl_sync(kFull, ro.s, 0);
+          rc = __shfl_sync(kFull, ro.rc, 0);
+          n_q += ro.nq;
+          if (rc) break;
+          if (s < dsub(cur_s, kTol) || s > dadd(nxt_s, kTol)) {
+            rc = kErrSplitBounds;
+            break;
+          }
+        }
+        {
+          const double lo = dadd(cur_s, 1e-15), hi = dsub(nxt_s, 1e-15);
+          s = (s < lo) ? lo : (hi < s) ? hi : s;
+        }
+        double x, y, z;
+        ray_point(g, s, x, y, z);
+        warp_query_setup(Q, c, x, y, z);
+        Q.dc = metric(x, y, z, pc);
+        Q.dn = metric(x, y, z, pn);
+        Q.cid = cur;
+        Q.nid = nxt;
+        Q.bound = dadd(fmax(Q.dc, Q.dn), 4.0 * kTol);
+        Q.G = guard_band(Q.bound, qe);
+        KnnList<3> r;
+        r.clear();
+        ++n_q;
+        bool good = warp_knn<3>(c, lane, Q, -1, r, s_node, s_mind, n_ver, n_steps);
+        if (!good || !knn3_decision_valid(r, Q.bound)) {
+          ++n_res;
+          good = warp_knn_unbounded<3>(c, lane, Q, qe, r, s_node, s_mind, n_ver, n_steps);
+          if (!good) {
+            // exact thread-level search by lane 0, broadcast
+            KnnList<3> t;
+            t.clear();
+            if (lane == 0) {
+              unsigned v = 0;
+              knn_exact64(c, x, y, z, pinf(), t, v);
+            }
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              r.r2[j] = __shfl_sync(kFull, t.r2[j], 0);
+              r.id[j] = __shfl_sync(kFull, t.id[j], 0);
+            }
+          }
+        }
+        if (r.id[0] < 0) {
+          rc = kErrNonFiniteDist;
+          break;
+        }
+        bool has_c = false, has_n = false, three_eq = true;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          if (dsub(r.r2[i], r.r2[0]) >= kTol) {
+            three_eq = false;
+            break;
+          }
+          if (r.id[i] == cur) has_c = true;
+          if (r.id[i] == nxt) has_n = true;
+        }
+        if (three_eq && !has_c && !has_n) {
+          RareOut ro{0.0, 0, 0, 0, 0u};
+          if (lane == 0) ro = rare_expand(c, x, y, z, cur, nxt);
+          rc = __shfl_sync(kFull, ro.rc, 0);
+          has_c = __shfl_sync(kFull, ro.a, 0);
+          has_n = __shfl_sync(kFull, ro.b, 0);
+          ++n_q;
+          if (rc) break;
+        }
+        if (has_c || has_n) {
+          emit(open_cell, entry_s, s);
+          open_cell = nxt;
+          entry_s = s;
+          --sp;
+          cur = nxt;
+          cur_s = nxt_s;
+          if (sp == 0) break;
+        } else if (dadd(r.r2[0], kTol) < r.r2[1]) {
+          if (sp >= kWWalkStack || sp >= io.local_cap) {
+            rc = kNeedSlow;
+            break;
+          }
+          if (lane == 0) {
+            w_id[sp] = r.id[0];
+            w_s[sp] = s;
+          }
+          ++sp;
+          __syncwarp();
+        } else {
+          RareOut ro{0.0, 0, 0, 0, 0u};
+          if (lane == 0) ro = rare_case1a(c, g, x, y, z, cur, nxt);
+          rc = __shfl_sync(kFull, ro.rc, 0);
+          const int sc = __shfl_sync(kFull, ro.a, 0), sn = __shfl_sync(kFull, ro.b, 0);
+          n_q += ro.nq;
+          if (rc) break;
+          const int need = sc == sn ? 1 : 2;
+          if (sp + need > kWWalkStack || sp + need > io.local_cap) {
+            rc = kNeedSlow;
+            break;
+          }
+          if (lane == 0) {
+            if (sc == sn) {
+              w_id[sp] = sc;
+              w_s[sp] = s;
+            } else {
+              w_id[sp] = sn;
+              w_s[sp] = s;
+              w_id[sp + 1] = sc;
+              w_s[sp + 1] = s;
+            }
+          }
+          sp += need;
+          __syncwarp();
+        }
+        max_sp = max(max_sp, (unsigned)sp);
+      }
+      if (rc == 0) emit(open_cell, entry_s, cur_s);
+    }
+    if (rc == 0) {
+      if (OUT == kOutImage || OUT == kOutCount) {
+        if (lane < io.nout) io.out[ray * io.nout + lane] = red.acc;
+        if (OUT == kOutCount && lane == 0) io.counts[ray] = red.nseg;
+      }
+      n_cross += nseg_now();
+    } else if (lane == 0) {
+      if (rc == kNeedSlow) hand_over(io, ray, nseg_now());
+      else report(io, ray, rc);
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    atomicAdd(&io.stats->rays, (unsigned long long)n_rays);
+    atomicAdd(&io.stats->crossings, (unsigned long long)n_cross);
+    atomicAdd(&io.stats->queries, (unsigned long long)n_q);
+    atomicAdd(&io.stats->fp64_resolves, (unsigned long long)n_res);
+    atomicMax(&io.stats->max_stack, (unsigned long long)max_sp);
+    atomicAdd(&io.stats->pad[0], (unsigned long long)n_steps);
+    atomicAdd(&io.stats->pad[1], (unsigned long long)n_ver);
+  }
+}
+
+template <int MODE, int OUT>
+int launch_warp(vt_cloud* cl, WalkIO& io, cudaStream_t st) {
+  const int B = kWarpsPerBlock * 32;
+  int dev = 0, nsms = 0;
+  VT_CUDA(cudaGetDevice(&dev));
+  VT_CUDA(cudaDeviceGetAttribute(&nsms, cudaDevAttrMultiProcessorCount, dev));
+  int per_sm = cl->blocks_per_sm;
+  if (per_sm <= 0) {
+    VT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_warp<MODE, OUT>, B, 0));
+    if (per_sm < 1) per_sm = 1;
+  }
+  int64_t blocks = (int64_t)nsms * per_sm;
+  const int64_t need = (io.nrays + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (blocks > need) blocks = need > 0 ? need : 1;
+  k_warp<MODE, OUT><<<(unsigned)blocks, B, 0, st>>>(cl->view, io);
+  return VT_OK;
+}
+
+}  // namespace vt
