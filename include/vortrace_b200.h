@@ -70,6 +70,8 @@ extern "C" {
                                   /* kernels' in-register stack before it is   */
                                   /* handed to the global-stack kernel         */
                                   /* (default and maximum: the compiled size)  */
+#define VT_PARAM_CACHE 8          /* batched kernel: per-ray neighbourhood     */
+                                  /* cache of the split-point queries (1, 0)   */
 
 typedef struct vt_cloud vt_cloud;
 typedef struct vt_segments vt_segments;
@@ -96,6 +98,10 @@ typedef struct {
   uint64_t slow_rays;     /* rays finished by the degenerate-geometry kernel */
   uint64_t max_stack;     /* deepest pending-point stack seen                */
   double walk_ms;         /* device time of the walk launch(es)               */
+  uint64_t search_steps;  /* node groups expanded (warp-cooperative search)  */
+  uint64_t fp64_checks;   /* FP64 re-checks of points passing the FP32 test  */
+  uint64_t cache_refreshes; /* neighbourhood-cache refills (batched kernel)  */
+  uint64_t cache_hits;    /* split queries answered from the cache           */
 } vt_stats;
 
 /* ---- library ----------------------------------------------------------- */

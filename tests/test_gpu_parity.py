@@ -228,3 +228,21 @@ def test_batch_projection_matches_individual(clustered):
         np.testing.assert_array_equal(img, pc.grid_projection(g["extent"], g["nres"],
                                                               g["bounds"], g["center"], **kw))
     np.testing.assert_array_equal(vals, pc.projection(rs, re_))
+
+
+def test_neighbourhood_cache_is_exact(clustered):
+    """The batched kernel's per-ray neighbourhood cache answers split queries
+    only when it provably holds every candidate: on/off give the same bits."""
+    from vortrace_b200 import _lib as L
+    w, pc, (lp, ot) = clustered
+    idx = np.linspace(0, len(w["starts"]) - 1, 8192).astype(np.int64)
+    S, E = w["starts"][idx], w["ends"][idx]
+    pc.kernel = "batched"
+    on = pc.projection(S, E)
+    assert pc.last_stats["cache_hits"] > 0
+    pc._cloud.set_param(L.PARAM_CACHE, 0)
+    off = pc.projection(S, E)
+    pc._cloud.set_param(L.PARAM_CACHE, 1)
+    assert pc.last_stats["cache_hits"] == 0
+    np.testing.assert_array_equal(on, off)
+    np.testing.assert_array_equal(on, ot.project(S, E))

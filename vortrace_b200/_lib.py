@@ -32,6 +32,7 @@ PARAM_SMEM_LEVELS = 4
 PARAM_BLOCKS_PER_SM = 5
 PARAM_LEAF_SIZE = 6
 PARAM_LOCAL_STACK = 7
+PARAM_CACHE = 8
 
 # every symbol the header declares (checked by the tests)
 EXPORTS = (
@@ -55,7 +56,9 @@ class CloudInfo(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("crossings", C.c_uint64), ("queries", C.c_uint64),
                 ("fp64_resolves", C.c_uint64), ("slow_rays", C.c_uint64),
-                ("max_stack", C.c_uint64), ("walk_ms", C.c_double)]
+                ("max_stack", C.c_uint64), ("walk_ms", C.c_double),
+                ("search_steps", C.c_uint64), ("fp64_checks", C.c_uint64),
+                ("cache_refreshes", C.c_uint64), ("cache_hits", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -300,6 +300,10 @@ int vt_cloud_set_param(vt_cloud* cl, int param, int64_t value) {
       if (value < 1) return set_error(VT_ERR_INVALID, "local stack size must be >= 1");
       cl->local_stack = value > (1 << 30) ? (1 << 30) : (int)value;
       return VT_OK;
+    case VT_PARAM_CACHE:
+      if (value < 0 || value > 1) return set_error(VT_ERR_INVALID, "cache mode must be 0 or 1");
+      cl->cache_mode = (int)value;
+      return VT_OK;
     case VT_PARAM_LEAF_SIZE:
       if (value < 2 || value > 64) return set_error(VT_ERR_INVALID, "leaf size out of range [2, 64]");
       cl->leaf_size = (int)value;

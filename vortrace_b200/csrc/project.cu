@@ -409,6 +409,7 @@ int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaS
   io.slow_threads = slow_threads;
   io.max_iter = cl->max_iter;
   io.local_cap = cl->local_stack;
+  io.cache_mode = cl->cache_mode;
   io.diag = nullptr;
   VT_CUDA(cudaMemsetAsync(io.stats, 0, sizeof(DevStats), st));
   VT_CUDA(cudaMemsetAsync(&io.stats->first_error, 0xff, sizeof(unsigned long long), st));
@@ -444,6 +445,10 @@ int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaS
     stats->slow_rays = hs.slow_rays;
     stats->max_stack = hs.max_stack;
     stats->walk_ms = ms;
+    stats->search_steps = hs.pad[0];
+    stats->fp64_checks = hs.pad[1];
+    stats->cache_refreshes = hs.pad[2];
+    stats->cache_hits = hs.pad[3];
   }
   if (hs.first_error != ~0ULL) {
     const int64_t ray = (int64_t)(hs.first_error >> 8);

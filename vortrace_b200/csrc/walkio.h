@@ -38,6 +38,7 @@ struct WalkIO {
   int slow_threads;
   int64_t max_iter;
   int local_cap;         // in-register stack entries per ray
+  int cache_mode;        // batched kernel: 1 = neighbourhood cache on
   WalkDiag* diag;
 };
 

@@ -36,7 +36,7 @@ constexpr int kWarpsPerBlock = 4;
 constexpr int kWSearchStack = 128;  // per-warp search stack entries
 constexpr int kWWalkStack = 64;     // per-warp pending ray points
 #ifndef VT_WARP_MINB
-#define VT_WARP_MINB 8
+#define VT_WARP_MINB 4
 #endif
 
 __device__ __forceinline__ float box_dist32(float q0, float q1, float q2, float4 lo, float4 hi) {
@@ -131,7 +131,7 @@ __device__ __forceinline__ void warp_leaves(const DevCloud& c, const int lane,
 // Returns false if the per-warp stack overflowed (the result is then not
 // trustworthy and the caller re-resolves the query).
 template <int K>
-__device__ bool warp_knn(const DevCloud& c, const int lane, const WarpQuery& Q,
+__device__ __forceinline__ bool warp_knn(const DevCloud& c, const int lane, const WarpQuery& Q,
                          const int64_t skip_leaf, KnnList<K>& L, int* s_node, float* s_mind,
                          unsigned& nver, unsigned& nsteps) {
   const int D = c.depth;
@@ -225,7 +225,7 @@ __device__ __forceinline__ int64_t warp_descend_leaf(const DevCloud& c, float q0
 // Unbounded K-NN: the leaf on the split-plane path first (all its points
 // are candidates), then a search bounded by the K-th best distance found.
 template <int K>
-__device__ bool warp_knn_unbounded(const DevCloud& c, const int lane, WarpQuery Q, double qe,
+__device__ __forceinline__ bool warp_knn_unbounded(const DevCloud& c, const int lane, WarpQuery Q, double qe,
                                    KnnList<K>& L, int* s_node, float* s_mind, unsigned& nver,
                                    unsigned& nsteps) {
   L.clear();
@@ -261,6 +261,198 @@ __device__ __forceinline__ void warp_query_setup(WarpQuery& Q, const DevCloud& c
   Q.q0 = __double2float_rn(dsub(x, c.origin[0]));
   Q.q1 = __double2float_rn(dsub(y, c.origin[1]));
   Q.q2 = __double2float_rn(dsub(z, c.origin[2]));
+}
+
+// ------------------------------------------------- neighbourhood cache
+// A per-warp cache of the points around a centre C on the ray:
+//   every point p with d64(C, p) < rho2 is in the cache (d64 = the FP64
+//   squared distance in the reference's operation order).
+// A split query (q, bound R) is answered from the cache when
+//   (sqrt(R) + sqrt(d64(q, C)))^2 * (1 + 1e-12) < rho2:
+// then |p - C| <= |p - q| + |q - C| for every p with d64(q, p) < R, so all
+// such points are cached, and the bounded 3-NN over the cache is the same
+// exact set as over the tree.  The factor covers the FP64 rounding of the
+// squared distances, square roots and sums (a few ulp each).
+constexpr int kCache = 128;  // points per warp (4 per lane)
+
+__device__ __forceinline__ bool cache_covers(double R, double dqc, double rho2) {
+  const double a = sqrt(R), b = sqrt(dqc);
+  const double t = (a + b) * (a + b);
+  return t * (1.0 + 1e-12) < rho2;
+}
+
+// Gather every point with d64(C, p) < rho2 into `cache` (FP32 coordinates,
+// tree index in .w).  Points beyond kCache are dropped and the guaranteed
+// radius shrinks to the smallest dropped distance; returns that radius^2
+// and the number cached.
+__device__ __forceinline__ double warp_gather(const DevCloud& c, const int lane,
+                                              const WarpQuery& C, double rho2, float4* cache,
+                                              int& count, int* s_node, float* s_mind,
+                                              unsigned& nver, unsigned& nsteps) {
+  const int D = c.depth;
+  const int64_t ninternal = c.nleaves - 1;
+  const float thr32 = __double2float_ru(dadd(rho2, C.G));
+  double mdrop = pinf();
+  count = 0;
+  int sp = 0;
+  int64_t gfirst;
+  int gm;
+  bool gleaves;
+  if (D == 0) {
+    gfirst = 0;
+    gm = 1;
+    gleaves = true;
+  } else {
+    const int s = ((D - 1) % 5) + 1;
+    gfirst = (1LL << s) - 1;
+    gm = 1 << s;
+    gleaves = (s == D);
+  }
+  for (;;) {
+    ++nsteps;
+    const int64_t node = gfirst + lane;
+    float nm = __int_as_float(0x7f800000);
+    bool surv = false;
+    if (lane < gm) {
+      nm = box_dist32(C.q0, C.q1, C.q2, __ldg(&c.boxlo[node]), __ldg(&c.boxhi[node]));
+      surv = nm < thr32;
+    }
+    const unsigned mask = __ballot_sync(kFull, surv);
+    bool next = false;
+    int v = 0;
+    if (gleaves) {
+      if (mask) {
+        int64_t a = 0;
+        int cnt = 0;
+        if (surv) {
+          const int64_t j = node - ninternal;
+          a = (j * c.n) >> D;
+          cnt = (int)((((j + 1) * c.n) >> D) - a);
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += t;
+        }
+        const int total = __shfl_sync(kFull, incl, 31);
+        for (int base = 0; base < total; base += 32) {
+          const int kk = base + lane;
+          int lo = 0, hi = 31;
+#pragma unroll
+          for (int it = 0; it < 5; ++it) {
+            const int mid = (lo + hi) >> 1;
+            if (__shfl_sync(kFull, incl, mid) > kk) hi = mid;
+            else lo = mid + 1;
+          }
+          const long long ao = __shfl_sync(kFull, (long long)a, lo);
+          const int exo = __shfl_sync(kFull, incl - cnt, lo);
+          const int64_t p = ao + (kk - exo);
+          const bool act = kk < total;
+          float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
+          float f = __int_as_float(0x7f800000);
+          if (act) {
+            P = __ldg(&c.pts32[p]);
+            f = pt_dist32(C.q0, C.q1, C.q2, P);
+          }
+          bool in = false;
+          double d = pinf();
+          if (act && f < thr32) {
+            d = metric(C.x, C.y, C.z, ldg_pt(&c.pts[p]));
+            ++nver;
+            in = d < rho2;
+          }
+          const unsigned im = __ballot_sync(kFull, in);
+          const int pos = count + __popc(im & ((1u << lane) - 1u));
+          if (in) {
+            if (pos < kCache) {
+              P.w = __int_as_float((int)p);
+              cache[pos] = P;
+            } else {
+              mdrop = fmin(mdrop, d);
+            }
+          }
+          count += __popc(im);
+        }
+      }
+    } else if (mask) {
+      const unsigned rest = mask & (mask - 1u);  // first survivor continues
+      const int cnt = __popc(rest);
+      if (sp + cnt > kWSearchStack) {
+        // no room to remember the other subtrees: they are not gathered,
+        // so the guarantee is void
+        mdrop = 0.0;
+      } else if ((rest >> lane) & 1u) {
+        const int e = sp + __popc(rest & ((1u << lane) - 1u));
+        s_node[e] = (int)node;
+      }
+      if (sp + cnt <= kWSearchStack) sp += cnt;
+      __syncwarp();
+      v = (int)(gfirst + __ffs(mask) - 1);
+      next = true;
+    }
+    if (!next) {
+      if (sp == 0) break;
+      v = s_node[--sp];
+      __syncwarp();
+    }
+    const int k = depth_of(v);
+    const int s = min(5, D - k);
+    gfirst = ((int64_t)(v + 1) << s) - 1;
+    gm = 1 << s;
+    gleaves = (k + s == D);
+  }
+  // all lanes agree on mdrop
+  mdrop = fmin(mdrop, __shfl_xor_sync(kFull, mdrop, 16));
+  mdrop = fmin(mdrop, __shfl_xor_sync(kFull, mdrop, 8));
+  mdrop = fmin(mdrop, __shfl_xor_sync(kFull, mdrop, 4));
+  mdrop = fmin(mdrop, __shfl_xor_sync(kFull, mdrop, 2));
+  mdrop = fmin(mdrop, __shfl_xor_sync(kFull, mdrop, 1));
+  if (count > kCache) count = kCache;
+  __syncwarp();
+  return fmin(rho2, mdrop);
+}
+
+// Bounded 3-NN over the cached points (same acceptance rule as warp_knn).
+__device__ __forceinline__ void warp_scan_cache(const DevCloud& c, const int lane,
+                                                const WarpQuery& Q, const float4* cache,
+                                                const int count, KnnList<3>& L,
+                                                unsigned& nver) {
+  L.clear();
+  double thr64 = Q.bound;
+  const float thr32 = __double2float_ru(dadd(thr64, Q.G));
+#pragma unroll
+  for (int j = 0; j < kCache / 32; ++j) {
+    const int idx = j * 32 + lane;
+    bool cand = false;
+    int p = -1;
+    if (idx < count) {
+      const float4 P = cache[idx];
+      p = __float_as_int(P.w);
+      cand = pt_dist32(Q.q0, Q.q1, Q.q2, P) < thr32;
+    }
+    unsigned cm = __ballot_sync(kFull, cand);
+    if (!cm) continue;
+    double d = 0.0;
+    if (cand) {
+      if (p == Q.cid) d = Q.dc;
+      else if (p == Q.nid) d = Q.dn;
+      else {
+        d = metric(Q.x, Q.y, Q.z, ldg_pt(&c.pts[p]));
+        ++nver;
+      }
+    }
+    while (cm) {
+      const int jj = __ffs(cm) - 1;
+      cm &= cm - 1;
+      const double dj = __shfl_sync(kFull, d, jj);
+      const int pj = __shfl_sync(kFull, p, jj);
+      if (dj < thr64) {
+        L.insert(dj, pj);
+        thr64 = fmin(Q.bound, L.worst());
+      }
+    }
+  }
 }
 
 // ------------------------------------------------------------------ sinks
@@ -341,14 +533,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
   __shared__ float s_mind_all[kWarpsPerBlock][kWSearchStack];
   __shared__ int w_id_all[kWarpsPerBlock][kWWalkStack];
   __shared__ double w_s_all[kWarpsPerBlock][kWWalkStack];
+  __shared__ float4 cache_all[kWarpsPerBlock][kCache];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   int* s_node = s_node_all[wib];
   float* s_mind = s_mind_all[wib];
   int* w_id = w_id_all[wib];
   double* w_s = w_s_all[wib];
+  float4* cache = cache_all[wib];
   const double cerr = (double)c.coord_err;
+  double cache_scale = 16.0;  // target cache radius^2 / R, adapted per warp
+  const bool use_cache = io.cache_mode != 0;
   unsigned n_rays = 0, n_cross = 0, n_q = 0, n_res = 0, n_ver = 0, n_steps = 0, max_sp = 0;
+  unsigned n_refresh = 0, n_hit = 0;
 
   for (;;) {
     long long ray = 0;
@@ -390,35 +587,29 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
       return (OUT == kOutImage || OUT == kOutCount) ? red.nseg : (OUT == kOutFill ? fill_n : adj.nseg);
     };
 
-    // ---- end cells
+    // ---- end cells: leaf on the split-plane path, then a bounded search
     WarpQuery Q;
-    Q.G = guard_band(1.0, qe);  // unbounded queries re-bound below
-    KnnList<1> r1;
-    int cend[2];
-    bool ok = true;
-    for (int e = 0; e < 2; ++e) {
-      const double* pt = e == 0 ? g.s : g.e;
-      warp_query_setup(Q, c, pt[0], pt[1], pt[2]);
-      // exact: the guard is re-derived from the leaf's best distance
+    auto nn_end = [&](double x, double y, double z) -> int {
+      warp_query_setup(Q, c, x, y, z);
+      KnnList<1> r1;
       r1.clear();
       const int64_t leaf = warp_descend_leaf(c, Q.q0, Q.q1, Q.q2);
-      {
-        const int64_t a = (leaf * c.n) >> c.depth;
-        const int cnt = (int)((((leaf + 1) * c.n) >> c.depth) - a);
-        for (int base = 0; base < cnt; base += 32) {
-          const int kk = base + lane;
-          double d = 0.0;
-          if (kk < cnt) d = metric(Q.x, Q.y, Q.z, ldg_pt(&c.pts[a + kk]));
-          const int m = min(32, cnt - base);
-          for (int j = 0; j < m; ++j) {
-            const double dj = __shfl_sync(kFull, d, j);
-            if (dj < r1.worst()) r1.insert(dj, (int)(a + base + j));
-          }
+      const int64_t a = (leaf * c.n) >> c.depth;
+      const int cnt = (int)((((leaf + 1) * c.n) >> c.depth) - a);
+      for (int base = 0; base < cnt; base += 32) {
+        const int kk = base + lane;
+        double d = 0.0;
+        if (kk < cnt) d = metric(x, y, z, ldg_pt(&c.pts[a + kk]));
+        const int m = min(32, cnt - base);
+        for (int j = 0; j < m; ++j) {
+          const double dj = __shfl_sync(kFull, d, j);
+          if (dj < r1.worst()) r1.insert(dj, (int)(a + base + j));
         }
       }
       Q.bound = pinf();
-      Q.G = guard_band(r1.worst(), qe);
+      Q.G = guard_band(r1.worst(), qe);  // the threshold never exceeds it
       Q.cid = Q.nid = -1;
+      Q.dc = Q.dn = 0.0;
       ++n_q;
       if (!warp_knn<1>(c, lane, Q, leaf, r1, s_node, s_mind, n_ver, n_steps)) {
         // search stack overflow: exact thread-level search by lane 0
@@ -426,26 +617,30 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
         int id = -1;
         if (lane == 0) {
           unsigned v = 0;
-          id = nn1_exact64(c, Q.x, Q.y, Q.z, v);
+          id = nn1_exact64(c, x, y, z, v);
         }
         r1.id[0] = __shfl_sync(kFull, id, 0);
       }
-      cend[e] = r1.id[0];
-      if (cend[e] < 0) ok = false;
-    }
-    if (!ok) {
+      return r1.id[0];
+    };
+    const int c0 = nn_end(g.s[0], g.s[1], g.s[2]);
+    const int c1 = nn_end(g.e[0], g.e[1], g.e[2]);
+    if (c0 < 0 || c1 < 0) {
       if (lane == 0) report(io, ray, kErrNonFiniteDist);
       continue;
     }
+    // neighbourhood cache of this ray (empty)
+    double cx = 0.0, cy = 0.0, cz = 0.0, rho2 = -1.0;
+    int ccount = 0;
     int rc = 0;
-    int cur = cend[0], open_cell = cend[0];
+    int cur = c0, open_cell = c0;
     double cur_s = 0.0, entry_s = 0.0;
-    if (cend[0] == cend[1]) {
-      emit(cend[0], 0.0, g.len);
+    if (c0 == c1) {
+      emit(c0, 0.0, g.len);
     } else {
       int sp = 1;
       if (lane == 0) {
-        w_id[0] = cend[1];
+        w_id[0] = c1;
         w_s[0] = g.len;
       }
       __syncwarp();
@@ -496,7 +691,34 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
         KnnList<3> r;
         r.clear();
         ++n_q;
-        bool good = warp_knn<3>(c, lane, Q, -1, r, s_node, s_mind, n_ver, n_steps);
+        bool good;
+        bool hit = false;
+        if (use_cache) {
+          double dqc = rho2 > 0.0 ? metric(x, y, z, make_double4(cx, cy, cz, 0.0)) : 0.0;
+          if (!(rho2 > 0.0 && cache_covers(Q.bound, dqc, rho2))) {
+            // refresh: centre ahead of the query on the ray
+            const double rt2 = cache_scale * Q.bound;
+            double sc = s + 0.5 * sqrt(rt2);
+            sc = sc > g.len ? g.len : sc;
+            WarpQuery Cq;
+            ray_point(g, sc, cx, cy, cz);
+            warp_query_setup(Cq, c, cx, cy, cz);
+            Cq.G = guard_band(rt2, qe);
+            rho2 = warp_gather(c, lane, Cq, rt2, cache, ccount, s_node, s_mind, n_ver, n_steps);
+            ++n_refresh;
+            // adapt the target radius to the cache's capacity
+            if (rho2 < rt2) cache_scale = fmax(2.0, cache_scale * 0.7);
+            else if (ccount < kCache / 3) cache_scale = fmin(256.0, cache_scale * 1.3);
+            dqc = metric(x, y, z, make_double4(cx, cy, cz, 0.0));
+          }
+          if (rho2 > 0.0 && cache_covers(Q.bound, dqc, rho2)) {
+            warp_scan_cache(c, lane, Q, cache, ccount, r, n_ver);
+            good = true;
+            hit = true;
+            ++n_hit;
+          }
+        }
+        if (!hit) good = warp_knn<3>(c, lane, Q, -1, r, s_node, s_mind, n_ver, n_steps);
         if (!good || !knn3_decision_valid(r, Q.bound)) {
           ++n_res;
           good = warp_knn_unbounded<3>(c, lane, Q, qe, r, s_node, s_mind, n_ver, n_steps);
@@ -607,6 +829,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
     atomicMax(&io.stats->max_stack, (unsigned long long)max_sp);
     atomicAdd(&io.stats->pad[0], (unsigned long long)n_steps);
     atomicAdd(&io.stats->pad[1], (unsigned long long)n_ver);
+    atomicAdd(&io.stats->pad[2], (unsigned long long)n_refresh);
+    atomicAdd(&io.stats->pad[3], (unsigned long long)n_hit);
   }
 }
 
