@@ -104,7 +104,7 @@ struct vt_cloud {
   int smem_levels = 9;
   int blocks_per_sm = 0;
   int local_stack = 1 << 30;  // capped to the compiled size in the kernels
-  int cache_mode = 1;
+  int cache_mode = 0;
   // device tree (tree order)
   vt::DevBuf<double4> pts_d;
   vt::DevBuf<float4> pts32_d;
