@@ -162,6 +162,24 @@ int vt_project_device(vt_cloud *cloud, const double *d_starts, const double *d_e
                       uint64_t nrays, int mode, int kernel, double *d_out, void *stream,
                       vt_stats *stats);
 
+/* No counterpart in the reference.  vt_project_device without any device
+ * allocation, for callers that cannot allocate device memory while they
+ * project: a framework whose caching allocator owns the device pool, or a
+ * latency-critical loop that cannot afford cudaMalloc/cudaFree and their
+ * implicit synchronisation.  Inputs and outputs are the caller's device
+ * buffers (starts/ends nrays x 3, out nrays x nout; kernel: the batched
+ * one); the walk's scratch is a fixed 8.9 MB static device array that every
+ * GPU loading the library holds until exit.  Limits: at most 1,048,576 rays
+ * per call (larger requests fail with VT_ERR_INVALID) and 512 pending ray
+ * points for rays handed to the global-stack kernel (VT_ERR_STACK beyond).
+ * The first call on a device looks up the scratch's device address; make
+ * that first call before any stream capture.  All calls share the one
+ * scratch array: calls that overlap on the GPU (other streams, other
+ * threads, other handles on the same device) race and must be serialised
+ * by the caller.  Returns after the launch has completed. */
+int vt_project_device_noalloc(vt_cloud *cloud, const double *d_starts, const double *d_ends,
+                              uint64_t nrays, int mode, double *d_out, void *stream);
+
 /* makeDetailedProjection + returnSegments (src/projection.cpp:75-144,
  * src/bindings.cpp:206-238).  Writes out (as vt_project) and the CSR
  * offsets (nrays + 1 entries), and returns a library-owned segment list

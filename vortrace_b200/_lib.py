@@ -40,7 +40,8 @@ EXPORTS = (
     "vt_set_warning_callback", "vt_set_device", "vt_cloud_create", "vt_cloud_build_tree",
     "vt_cloud_set_param", "vt_cloud_set_fields", "vt_cloud_set_fields_device",
     "vt_cloud_get_info", "vt_cloud_orig_ids", "vt_cloud_destroy", "vt_knn",
-    "vt_project", "vt_project_device", "vt_project_detailed", "vt_segments_count",
+    "vt_project", "vt_project_device", "vt_project_device_noalloc", "vt_project_detailed",
+    "vt_segments_count",
     "vt_segments_copy", "vt_segments_free", "vt_project_adjoint", "vt_project_adjoint_device",
 )
 
@@ -114,6 +115,7 @@ def load(path: str | None = None):
         L.vt_project.argtypes = [vp, dp, dp, u64, C.c_int, C.c_int, dp, C.POINTER(Stats)]
         L.vt_project_device.argtypes = [vp, vp, vp, u64, C.c_int, C.c_int, vp, vp,
                                         C.POINTER(Stats)]
+        L.vt_project_device_noalloc.argtypes = [vp, vp, vp, u64, C.c_int, vp, vp]
         L.vt_project_detailed.argtypes = [vp, dp, dp, u64, C.c_int, dp, i64p, C.POINTER(vp)]
         L.vt_segments_count.argtypes = [vp]
         L.vt_segments_count.restype = u64
@@ -125,7 +127,8 @@ def load(path: str | None = None):
         for name in ("vt_cloud_create", "vt_cloud_build_tree", "vt_cloud_set_param",
                      "vt_cloud_set_fields", "vt_cloud_set_fields_device",
                      "vt_cloud_get_info", "vt_cloud_orig_ids", "vt_knn", "vt_project",
-                     "vt_project_device", "vt_project_detailed", "vt_segments_copy",
+                     "vt_project_device", "vt_project_device_noalloc", "vt_project_detailed",
+                     "vt_segments_copy",
                      "vt_project_adjoint", "vt_project_adjoint_device", "vt_set_device"):
             getattr(L, name).restype = C.c_int
         L.vt_set_warning_callback(_warn_cb)

@@ -46,6 +46,7 @@ void warn(const std::string& msg) {
 bool verbose() { return g_verbose.load(); }
 }  // namespace vt
 
+using vt::check_projectable;
 using vt::set_error;
 
 #define VT_GUARD_BEGIN try {
@@ -58,7 +59,7 @@ using vt::set_error;
     return set_error(VT_ERR_RUNTIME, e.what());                           \
   }
 
-static int check_projectable(const vt_cloud* cl, int mode) {
+int vt::check_projectable(const vt_cloud* cl, int mode) {
   if (!cl) return set_error(VT_ERR_INVALID, "null cloud handle");
   if (!cl->tree_built)
     return set_error(VT_ERR_RUNTIME, "There is currently no valid tree for this point cloud");

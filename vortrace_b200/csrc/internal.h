@@ -128,4 +128,6 @@ struct vt_cloud {
 namespace vt {
 int build_tree_device(vt_cloud* cl);
 int upload_fields(vt_cloud* cl, const double* src, bool src_device, cudaStream_t st);
+// tree built, mode valid, volume needs valid RGBA (src/reduction.cpp:59-66)
+int check_projectable(const vt_cloud* cl, int mode);
 }

@@ -392,31 +392,25 @@ static std::string fmt_double(double v) {
   return buf;
 }
 
-// Run one walk launch (+ handed-over rays) and turn a per-ray failure into
-// the reference's error message.
-int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaStream_t st,
-             vt_stats* stats) {
-  const int slow_threads = 1024;
-  if (cl->ws_stats.reserve(1)) return VT_ERR_NOMEM;
-  if (cl->ws_slow.reserve(io.nrays > 0 ? io.nrays : 1)) return VT_ERR_NOMEM;
-  if (cl->ws_stack_id.reserve((size_t)slow_threads * cl->stack_cap)) return VT_ERR_NOMEM;
-  if (cl->ws_stack_s.reserve((size_t)slow_threads * cl->stack_cap)) return VT_ERR_NOMEM;
-  io.stats = cl->ws_stats.p;
-  io.slow_q = cl->ws_slow.p;
-  io.gstack_id = cl->ws_stack_id.p;
-  io.gstack_s = cl->ws_stack_s.p;
-  io.gstack_cap = cl->stack_cap;
-  io.slow_threads = slow_threads;
+// One walk launch (+ handed-over rays) on scratch already placed in `io`
+// (stats, hand-over queue, global stacks); turns a per-ray failure into the
+// reference's error message.  `d_diag`: device scratch for the diagnosis of
+// a failing ray (NULL: allocated on demand).  `timed`: CUDA events around
+// the launches for vt_stats.walk_ms.
+static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel,
+                       cudaStream_t st, vt_stats* stats, WalkDiag* d_diag, bool timed) {
   io.max_iter = cl->max_iter;
   io.local_cap = cl->local_stack;
   io.cache_mode = cl->cache_mode;
   io.diag = nullptr;
   VT_CUDA(cudaMemsetAsync(io.stats, 0, sizeof(DevStats), st));
   VT_CUDA(cudaMemsetAsync(&io.stats->first_error, 0xff, sizeof(unsigned long long), st));
-  cudaEvent_t e0, e1;
-  VT_CUDA(cudaEventCreate(&e0));
-  VT_CUDA(cudaEventCreate(&e1));
-  VT_CUDA(cudaEventRecord(e0, st));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (timed) {
+    VT_CUDA(cudaEventCreate(&e0));
+    VT_CUDA(cudaEventCreate(&e1));
+    VT_CUDA(cudaEventRecord(e0, st));
+  }
   int rc;
   switch (out_kind) {
     case kOutImage: rc = launch_walk_mode<kOutImage>(cl, io, mode, kernel, st); break;
@@ -425,18 +419,22 @@ int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaS
     default: rc = launch_walk_mode<kOutAdj>(cl, io, mode, kernel, st); break;
   }
   if (rc) {
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    if (timed) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+    }
     return rc;
   }
-  VT_CUDA(cudaEventRecord(e1, st));
+  if (timed) VT_CUDA(cudaEventRecord(e1, st));
   DevStats hs;
   VT_CUDA(cudaMemcpyAsync(&hs, io.stats, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
   VT_CUDA(cudaStreamSynchronize(st));
   float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (timed) {
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
   if (stats) {
     stats->rays = hs.rays;
     stats->crossings = hs.crossings;
@@ -455,13 +453,16 @@ int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaS
     const int code = (int)(hs.first_error & 0xff);
     // re-walk the failing ray alone for the message details
     DevBuf<WalkDiag> dg;
-    if (dg.alloc(1)) return VT_ERR_NOMEM;
+    if (!d_diag) {
+      if (dg.alloc(1)) return VT_ERR_NOMEM;
+      d_diag = dg.p;
+    }
     WalkDiag hd{0, -1, -1, 0.0, 0.0, 0.0};
-    VT_CUDA(cudaMemcpyAsync(dg.p, &hd, sizeof(hd), cudaMemcpyHostToDevice, st));
-    io.diag = dg.p;
+    VT_CUDA(cudaMemcpyAsync(d_diag, &hd, sizeof(hd), cudaMemcpyHostToDevice, st));
+    io.diag = d_diag;
     k_diag<<<1, 1, 0, st>>>(cl->view, io, ray);
     VT_CUDA(cudaGetLastError());
-    VT_CUDA(cudaMemcpyAsync(&hd, dg.p, sizeof(hd), cudaMemcpyDeviceToHost, st));
+    VT_CUDA(cudaMemcpyAsync(&hd, d_diag, sizeof(hd), cudaMemcpyDeviceToHost, st));
     VT_CUDA(cudaStreamSynchronize(st));
     io.diag = nullptr;
     std::string msg;
@@ -487,7 +488,7 @@ int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaS
         break;
       case kErrStack:
         msg = "Ray walk exceeded the pending-point stack capacity (" +
-              std::to_string(cl->stack_cap) + ")";
+              std::to_string(io.gstack_cap) + ")";
         break;
       case kErrNonFinite:
         return set_error(VT_ERR_INVALID,
@@ -500,6 +501,23 @@ int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaS
     return set_error(code, msg);
   }
   return VT_OK;
+}
+
+// Walk launch with the handle's (grow-only) workspace as scratch.
+int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaStream_t st,
+             vt_stats* stats) {
+  const int slow_threads = 1024;
+  if (cl->ws_stats.reserve(1)) return VT_ERR_NOMEM;
+  if (cl->ws_slow.reserve(io.nrays > 0 ? io.nrays : 1)) return VT_ERR_NOMEM;
+  if (cl->ws_stack_id.reserve((size_t)slow_threads * cl->stack_cap)) return VT_ERR_NOMEM;
+  if (cl->ws_stack_s.reserve((size_t)slow_threads * cl->stack_cap)) return VT_ERR_NOMEM;
+  io.stats = cl->ws_stats.p;
+  io.slow_q = cl->ws_slow.p;
+  io.gstack_id = cl->ws_stack_id.p;
+  io.gstack_s = cl->ws_stack_s.p;
+  io.gstack_cap = cl->stack_cap;
+  io.slow_threads = slow_threads;
+  return run_walk_on(cl, io, out_kind, mode, kernel, st, stats, nullptr, true);
 }
 
 int run_knn(vt_cloud* cl, const double* d_q, int64_t nq, int k, int64_t* d_ids, double* d_r2,
@@ -523,3 +541,93 @@ int scan_offsets(vt_cloud* cl, const int64_t* d_counts, int64_t* d_offsets, int6
 }
 
 }  // namespace vt
+
+namespace vt {
+
+// ------------------------------------------- projection without allocation
+// Some callers cannot allocate device memory while they run projections: a
+// framework whose caching allocator owns the device pool (a cudaMalloc of
+// ours would bypass its budget or fail), or a latency-critical loop where
+// cudaMalloc/cudaFree and their implicit device synchronisation are not
+// acceptable.  vt_project_device_noalloc serves them: the walk's scratch
+// (counters and work-queue head, the first-error slot, the diagnosis record,
+// the hand-over queue and the global-memory stacks of k_slow) lives in the
+// file-scope array below, which every GPU that loads the library holds
+// until the process exits.  The cloud and its tree are allocated earlier,
+// by vt_cloud_create / vt_cloud_build_tree.
+constexpr int64_t kNoAllocMaxRays = 1LL << 20;  // hand-over queue slots (1 per ray)
+constexpr int kNoAllocSlowThreads = 128;       // threads of k_slow
+constexpr int kNoAllocStackCap = 512;          // pending points per handed-over ray
+constexpr size_t kNoAllocOffStats = 0;
+constexpr size_t kNoAllocOffDiag = 256;
+constexpr size_t kNoAllocOffQueue = 512;
+constexpr size_t kNoAllocOffStackId = kNoAllocOffQueue + (size_t)kNoAllocMaxRays * 8;
+constexpr size_t kNoAllocOffStackS =
+    kNoAllocOffStackId + (size_t)kNoAllocSlowThreads * kNoAllocStackCap * 4;
+constexpr size_t kNoAllocBytes =
+    kNoAllocOffStackS + (size_t)kNoAllocSlowThreads * kNoAllocStackCap * 8;  // 8.9 MB
+static_assert(sizeof(DevStats) <= 256 && sizeof(WalkDiag) <= 256, "scratch layout");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch, looked up once per device with that
+// device current (the host-side symbol is not a device address).
+static std::mutex g_noalloc_mu;
+static unsigned char* g_noalloc_ptr[128] = {};
+
+static int noalloc_scratch(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= 128) return set_error(VT_ERR_INVALID, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return set_error(VT_ERR_CUDA, std::string("cudaGetSymbolAddress of the no-allocation "
+                                                "scratch failed: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = (unsigned char*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return VT_OK;
+}
+
+}  // namespace vt
+
+extern "C" int vt_project_device_noalloc(vt_cloud* cl, const double* d_starts,
+                                         const double* d_ends, uint64_t nrays, int mode,
+                                         double* d_out, void* stream) {
+  using namespace vt;
+  try {
+    int rc = check_projectable(cl, mode);
+    if (rc) return rc;
+    if (nrays > (uint64_t)kNoAllocMaxRays)
+      return set_error(VT_ERR_INVALID,
+                       "vt_project_device_noalloc: " + std::to_string(nrays) +
+                           " rays exceed the no-allocation limit of " +
+                           std::to_string(kNoAllocMaxRays) + " rays per call");
+    std::lock_guard<std::mutex> lk(cl->mu);
+    VT_CUDA(cudaSetDevice(cl->device));
+    if (nrays == 0) return VT_OK;
+    unsigned char* base = nullptr;
+    if ((rc = noalloc_scratch(cl->device, &base))) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : cl->stream;
+    WalkIO io{};
+    io.starts = d_starts;
+    io.ends = d_ends;
+    io.nrays = (int64_t)nrays;
+    io.nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
+    io.out = d_out;
+    io.stats = reinterpret_cast<DevStats*>(base + kNoAllocOffStats);
+    io.slow_q = reinterpret_cast<unsigned long long*>(base + kNoAllocOffQueue);
+    io.gstack_id = reinterpret_cast<int*>(base + kNoAllocOffStackId);
+    io.gstack_s = reinterpret_cast<double*>(base + kNoAllocOffStackS);
+    io.gstack_cap = cl->stack_cap < kNoAllocStackCap ? cl->stack_cap : kNoAllocStackCap;
+    io.slow_threads = kNoAllocSlowThreads;
+    // counters and the first-error slot are cleared by run_walk_on; the
+    // queue and stacks need no clearing (written before they are read)
+    return run_walk_on(cl, io, kOutImage, mode, VT_KERNEL_BATCHED, st, nullptr,
+                       reinterpret_cast<WalkDiag*>(base + kNoAllocOffDiag), false);
+  } catch (const std::exception& e) {
+    return set_error(VT_ERR_RUNTIME, e.what());
+  }
+}
+
