@@ -263,38 +263,86 @@ __device__ __forceinline__ void warp_query_setup(WarpQuery& Q, const DevCloud& c
   Q.q2 = __double2float_rn(dsub(z, c.origin[2]));
 }
 
-// ------------------------------------------------- neighbourhood cache
-// A per-warp cache of the points around a centre C on the ray:
-//   every point p with d64(C, p) < rho2 is in the cache (d64 = the FP64
-//   squared distance in the reference's operation order).
-// A split query (q, bound R) is answered from the cache when
-//   (sqrt(R) + sqrt(d64(q, C)))^2 * (1 + 1e-12) < rho2:
-// then |p - C| <= |p - q| + |q - C| for every p with d64(q, p) < R, so all
-// such points are cached, and the bounded 3-NN over the cache is the same
-// exact set as over the tree.  The factor covers the FP64 rounding of the
-// squared distances, square roots and sums (a few ulp each).
-constexpr int kCache = 128;  // points per warp (4 per lane)
+// ------------------------------------------------- capsule cache
+// Consecutive split points of a ray lie on the ray and move forward (a
+// query's s is never below the walk's current s), so one gather of the
+// points around a stretch of the ray serves many queries.  A warp keeps a
+// "capsule" of points:
+//   every point p whose axial parameter t = (p - P_a).dir lies in [0, L]
+//   and whose distance from the ray's line is < rho is in the cache,
+// with P_a = start + s_a dir.  A split query at parameter s with bound R is
+// answered from the cache when r = sqrt(R)(1 + 1e-12) + eps satisfies
+// r <= rho and s_a <= s - r and s + r <= s_a + L: every p with
+// d64(q, p) < R has |t(p) - (s - s_a)| <= |p - q| < r and a distance from
+// the line below r <= rho, so it is cached, and the bounded 3-NN over the
+// cache is the same exact set as over the tree.  The gather's membership
+// test runs in FP64 on the FP64 points; eps covers FP64 rounding.
+#ifndef VT_WARP_CACHE
+#define VT_WARP_CACHE 64
+#endif
+constexpr int kCache = VT_WARP_CACHE;  // points per warp
 
-__device__ __forceinline__ bool cache_covers(double R, double dqc, double rho2) {
-  const double a = sqrt(R), b = sqrt(dqc);
-  const double t = (a + b) * (a + b);
-  return t * (1.0 + 1e-12) < rho2;
+struct Capsule {
+  double sa, L, rho;  // start parameter, guaranteed length and radius
+  int count;
+};
+
+__device__ __forceinline__ bool capsule_covers(const Capsule& K, double s, double R,
+                                               double eps) {
+  const double r = sqrt(R) * (1.0 + 1e-12) + eps;
+  const double t = s - K.sa;
+  return r <= K.rho && t - r >= 0.0 && t + r <= K.L;
 }
 
-// Gather every point with d64(C, p) < rho2 into `cache` (FP32 coordinates,
-// tree index in .w).  Points beyond kCache are dropped and the guaranteed
-// radius shrinks to the smallest dropped distance; returns that radius^2
-// and the number cached.
-__device__ __forceinline__ double warp_gather(const DevCloud& c, const int lane,
-                                              const WarpQuery& C, double rho2, float4* cache,
-                                              int& count, int* s_node, float* s_mind,
-                                              unsigned& nver, unsigned& nsteps) {
+// Does the segment P0 + t d, t in [t0, t1], come within w (per axis) of the
+// box [lo, hi]?  A necessary condition for any point of the box to lie
+// within distance w of the segment.
+__device__ __forceinline__ bool seg_near_box(const double P0[3], const double d[3],
+                                             const double invd[3], double t0, double t1,
+                                             float4 lo, float4 hi, double w) {
+  const double l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z};
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const double l = l3[j] - w - P0[j], h = h3[j] + w - P0[j];
+    if (d[j] == 0.0) {
+      if (l > 0.0 || h < 0.0) return false;
+    } else {
+      double a = l * invd[j], b = h * invd[j];
+      if (a > b) {
+        const double x = a;
+        a = b;
+        b = x;
+      }
+      t0 = fmax(t0, a);
+      t1 = fmin(t1, b);
+    }
+  }
+  return t0 <= t1 + 1e-9;
+}
+
+// Gather the capsule (start parameter sa, length L, radius rho) of ray g.
+__device__ __forceinline__ Capsule warp_gather_capsule(const DevCloud& c, const int lane,
+                                                       const RayGeom& g, double sa, double L,
+                                                       double rho, double eps, float4* cache,
+                                                       int* s_node, unsigned& nver,
+                                                       unsigned& nsteps) {
   const int D = c.depth;
   const int64_t ninternal = c.nleaves - 1;
-  const float thr32 = __double2float_ru(dadd(rho2, C.G));
-  double mdrop = pinf();
-  count = 0;
+  double Pa[3], P0[3], invd[3];
+  ray_point(g, sa, Pa[0], Pa[1], Pa[2]);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    P0[j] = Pa[j] - c.origin[j];  // frame of the node boxes
+    invd[j] = g.d[j] != 0.0 ? 1.0 / g.d[j] : 0.0;
+  }
+  // node boxes bound the FP32 images; real points are within coord_err
+  const double wbox = rho + (double)c.coord_err + eps;
+  const double t_lo = -eps, t_hi = L + eps;
+  const double rho2_in = rho * rho * (1.0 + 1e-12) + eps * eps;
+  double tdrop = pinf();
+  int count = 0;
   int sp = 0;
+  bool lost = false;
   int64_t gfirst;
   int gm;
   bool gleaves;
@@ -311,12 +359,10 @@ __device__ __forceinline__ double warp_gather(const DevCloud& c, const int lane,
   for (;;) {
     ++nsteps;
     const int64_t node = gfirst + lane;
-    float nm = __int_as_float(0x7f800000);
     bool surv = false;
-    if (lane < gm) {
-      nm = box_dist32(C.q0, C.q1, C.q2, __ldg(&c.boxlo[node]), __ldg(&c.boxhi[node]));
-      surv = nm < thr32;
-    }
+    if (lane < gm)
+      surv = seg_near_box(P0, g.d, invd, t_lo, t_hi, __ldg(&c.boxlo[node]),
+                          __ldg(&c.boxhi[node]), wbox);
     const unsigned mask = __ballot_sync(kFull, surv);
     bool next = false;
     int v = 0;
@@ -348,28 +394,25 @@ __device__ __forceinline__ double warp_gather(const DevCloud& c, const int lane,
           const long long ao = __shfl_sync(kFull, (long long)a, lo);
           const int exo = __shfl_sync(kFull, incl - cnt, lo);
           const int64_t p = ao + (kk - exo);
-          const bool act = kk < total;
-          float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
-          float f = __int_as_float(0x7f800000);
-          if (act) {
-            P = __ldg(&c.pts32[p]);
-            f = pt_dist32(C.q0, C.q1, C.q2, P);
-          }
           bool in = false;
-          double d = pinf();
-          if (act && f < thr32) {
-            d = metric(C.x, C.y, C.z, ldg_pt(&c.pts[p]));
+          double tp = 0.0;
+          if (kk < total) {
+            const double4 P = ldg_pt(&c.pts[p]);
+            const double ax = P.x - Pa[0], ay = P.y - Pa[1], az = P.z - Pa[2];
+            tp = ax * g.d[0] + ay * g.d[1] + az * g.d[2];
+            const double rx = ax - tp * g.d[0], ry = ay - tp * g.d[1], rz = az - tp * g.d[2];
+            in = tp >= t_lo && tp <= t_hi && rx * rx + ry * ry + rz * rz < rho2_in;
             ++nver;
-            in = d < rho2;
           }
           const unsigned im = __ballot_sync(kFull, in);
           const int pos = count + __popc(im & ((1u << lane) - 1u));
           if (in) {
             if (pos < kCache) {
-              P.w = __int_as_float((int)p);
-              cache[pos] = P;
+              float4 P32 = __ldg(&c.pts32[p]);
+              P32.w = __int_as_float((int)p);
+              cache[pos] = P32;
             } else {
-              mdrop = fmin(mdrop, d);
+              tdrop = fmin(tdrop, tp);
             }
           }
           count += __popc(im);
@@ -379,14 +422,11 @@ __device__ __forceinline__ double warp_gather(const DevCloud& c, const int lane,
       const unsigned rest = mask & (mask - 1u);  // first survivor continues
       const int cnt = __popc(rest);
       if (sp + cnt > kWSearchStack) {
-        // no room to remember the other subtrees: they are not gathered,
-        // so the guarantee is void
-        mdrop = 0.0;
-      } else if ((rest >> lane) & 1u) {
-        const int e = sp + __popc(rest & ((1u << lane) - 1u));
-        s_node[e] = (int)node;
+        lost = true;  // subtrees not remembered: no guarantee
+      } else {
+        if ((rest >> lane) & 1u) s_node[sp + __popc(rest & ((1u << lane) - 1u))] = (int)node;
+        sp += cnt;
       }
-      if (sp + cnt <= kWSearchStack) sp += cnt;
       __syncwarp();
       v = (int)(gfirst + __ffs(mask) - 1);
       next = true;
@@ -402,15 +442,16 @@ __device__ __forceinline__ double warp_gather(const DevCloud& c, const int lane,
     gm = 1 << s;
     gleaves = (k + s == D);
   }
-  // all lanes agree on mdrop
-  mdrop = fmin(mdrop, __shfl_xor_sync(kFull, mdrop, 16));
-  mdrop = fmin(mdrop, __shfl_xor_sync(kFull, mdrop, 8));
-  mdrop = fmin(mdrop, __shfl_xor_sync(kFull, mdrop, 4));
-  mdrop = fmin(mdrop, __shfl_xor_sync(kFull, mdrop, 2));
-  mdrop = fmin(mdrop, __shfl_xor_sync(kFull, mdrop, 1));
-  if (count > kCache) count = kCache;
+  // all lanes agree on the smallest dropped parameter
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) tdrop = fmin(tdrop, __shfl_xor_sync(kFull, tdrop, o));
   __syncwarp();
-  return fmin(rho2, mdrop);
+  Capsule K;
+  K.sa = sa;
+  K.rho = rho;
+  K.count = count < kCache ? count : kCache;
+  K.L = lost ? -1.0 : fmin(L, tdrop - 2.0 * eps);
+  return K;
 }
 
 // Bounded 3-NN over the cached points (same acceptance rule as warp_knn).
@@ -542,7 +583,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
   double* w_s = w_s_all[wib];
   float4* cache = cache_all[wib];
   const double cerr = (double)c.coord_err;
-  double cache_scale = 16.0;  // target cache radius^2 / R, adapted per warp
+  double cap_lambda = 12.0;  // capsule length / radius, adapted per warp
   const bool use_cache = io.cache_mode != 0;
   unsigned n_rays = 0, n_cross = 0, n_q = 0, n_res = 0, n_ver = 0, n_steps = 0, max_sp = 0;
   unsigned n_refresh = 0, n_hit = 0;
@@ -629,9 +670,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
       if (lane == 0) report(io, ray, kErrNonFiniteDist);
       continue;
     }
-    // neighbourhood cache of this ray (empty)
-    double cx = 0.0, cy = 0.0, cz = 0.0, rho2 = -1.0;
-    int ccount = 0;
+    // capsule cache of this ray (empty)
+    Capsule cap;
+    cap.sa = 0.0;
+    cap.L = -1.0;
+    cap.rho = 0.0;
+    cap.count = 0;
+    // absolute FP64 slack of the capsule tests (a few ulp of the coordinates)
+    const double cap_eps = 1e-12 * (qe / 6.0e-8 + g.len + 1.0);
     int rc = 0;
     int cur = c0, open_cell = c0;
     double cur_s = 0.0, entry_s = 0.0;
@@ -694,25 +740,22 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
         bool good;
         bool hit = false;
         if (use_cache) {
-          double dqc = rho2 > 0.0 ? metric(x, y, z, make_double4(cx, cy, cz, 0.0)) : 0.0;
-          if (!(rho2 > 0.0 && cache_covers(Q.bound, dqc, rho2))) {
-            // refresh: centre ahead of the query on the ray
-            const double rt2 = cache_scale * Q.bound;
-            double sc = s + 0.5 * sqrt(rt2);
-            sc = sc > g.len ? g.len : sc;
-            WarpQuery Cq;
-            ray_point(g, sc, cx, cy, cz);
-            warp_query_setup(Cq, c, cx, cy, cz);
-            Cq.G = guard_band(rt2, qe);
-            rho2 = warp_gather(c, lane, Cq, rt2, cache, ccount, s_node, s_mind, n_ver, n_steps);
+          const double rho = 1.5 * sqrt(Q.bound);
+          // refresh only for queries a capsule starting at the walk's current
+          // point can reach (far split points of the bisection phase are
+          // searched in the tree directly)
+          if (!capsule_covers(cap, s, Q.bound, cap_eps) &&
+              s - cur_s <= (cap_lambda - 2.2) * rho) {
+            // radius 1.5 sqrt(R), starting rho before the walk's current
+            // point (later queries never lie behind it)
+            cap = warp_gather_capsule(c, lane, g, cur_s - rho, cap_lambda * rho, rho, cap_eps,
+                                      cache, s_node, n_ver, n_steps);
             ++n_refresh;
-            // adapt the target radius to the cache's capacity
-            if (rho2 < rt2) cache_scale = fmax(2.0, cache_scale * 0.7);
-            else if (ccount < kCache / 3) cache_scale = fmin(256.0, cache_scale * 1.3);
-            dqc = metric(x, y, z, make_double4(cx, cy, cz, 0.0));
+            if (cap.L < cap_lambda * rho) cap_lambda = fmax(4.0, cap_lambda * 0.75);
+            else if (cap.count < kCache / 2) cap_lambda = fmin(400.0, cap_lambda * 1.25);
           }
-          if (rho2 > 0.0 && cache_covers(Q.bound, dqc, rho2)) {
-            warp_scan_cache(c, lane, Q, cache, ccount, r, n_ver);
+          if (capsule_covers(cap, s, Q.bound, cap_eps)) {
+            warp_scan_cache(c, lane, Q, cache, cap.count, r, n_ver);
             good = true;
             hit = true;
             ++n_hit;
