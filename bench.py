@@ -9,8 +9,10 @@ cloud and its device tree are built once, outside the timed region, as the
 reference's timing of Projection::makeProjection excludes buildTree).
 Prints one JSON line (rank 0).
 
-Metric: cell crossings per second (Mcrossings/s) of the batched guarded-FP32
-kernel, forward; the same line reports forward+adjoint and the plain FP64
+Metric: cell crossings per second (Mcrossings/s) of the batched kernel
+(VT_KERNEL_AUTO: persistent, one ray per thread, rays in a coherent sorted
+order, bounded exact k-NN), forward; the same line reports forward+adjoint,
+the guarded-FP32 variant of the batched kernel and the plain FP64
 one-ray-per-thread kernel.  Multi-GPU (torchrun): every rank projects its own
 view of the cloud (the grid rotated about the cloud centre by 2*pi*rank/N):
 weak scaling, no data-path collective; value = all ranks' crossings / max
@@ -291,38 +293,46 @@ def run_ours(args):
         return float(t.item())
 
     K, W = args.steps, args.warmup
-    # --- forward, batched guarded-FP32 kernel (the headline)
+    # --- forward, batched kernel (the headline)
     for _ in range(W):
-        fwd(L.KERNEL_BATCHED)
+        fwd(L.KERNEL_AUTO)
     barrier()
     sampler = ClockSampler(local)
     sampler.start()
     walk_ms = []
 
     def f_b():
-        c, wm, _, _ = fwd(L.KERNEL_BATCHED)
+        c, wm, _, _ = fwd(L.KERNEL_AUTO)
         walk_ms.append(wm)
 
     fwd_ms = timed(f_b, K)
     barrier()
     clocks = sampler.stop()
-    crossings, _, resolves, queries = fwd(L.KERNEL_BATCHED)
+    crossings, _, resolves, queries = fwd(L.KERNEL_AUTO)
     t_fwd = reduce_max(sum(fwd_ms))
     tot_cross = reduce_sum(float(crossings))
     value = tot_cross * K / (t_fwd / 1e3) / 1e6
 
     # --- forward + adjoint
     for _ in range(max(1, W // 2)):
-        fwd(L.KERNEL_BATCHED)
+        fwd(L.KERNEL_AUTO)
         bwd()
     barrier()
-    fb_ms = timed(lambda: (fwd(L.KERNEL_BATCHED), bwd()), K)
+    fb_ms = timed(lambda: (fwd(L.KERNEL_AUTO), bwd()), K)
     barrier()
     t_fb = reduce_max(sum(fb_ms))
     fb_value = tot_cross * K / (t_fb / 1e3) / 1e6
 
-    # --- plain FP64 one-ray-per-thread kernel (the baseline kernel)
+    # --- the batched kernel with the guarded-FP32 k-NN
     kp = max(2, K // 2)
+    fwd(L.KERNEL_THREAD_FP32)
+    barrier()
+    g32_ms = timed(lambda: fwd(L.KERNEL_THREAD_FP32), kp)
+    barrier()
+    t_g32 = reduce_max(sum(g32_ms))
+    g32_value = tot_cross * kp / (t_g32 / 1e3) / 1e6
+
+    # --- plain FP64 one-ray-per-thread kernel (the baseline kernel)
     fwd(L.KERNEL_PLAIN_FP64)
     barrier()
     pl_ms = timed(lambda: fwd(L.KERNEL_PLAIN_FP64), kp)
@@ -377,7 +387,7 @@ def run_ours(args):
         roof = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "peak_source": peak_src, "bytes_per_crossing": bx,
-                "kernel": "k_batched (guarded FP32)"}
+                "kernel": "k_batched (bounded FP64 k-NN, coherent ray order)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -402,6 +412,8 @@ def run_ours(args):
                        "tree_build_ms": round(info.tree_build_ms, 2),
                        "parallelism": f"rays sharded by view, {world} rank(s)"},
             "fwd_bwd_mcrossings_per_s": round(fb_value, 4),
+            "kernel": "batched (VT_KERNEL_AUTO = VT_KERNEL_BATCHED_FP64)",
+            "guarded_fp32_mcrossings_per_s": round(g32_value, 4),
             "plain_fp64_mcrossings_per_s": round(pl_value, 4),
             "speedup_vs_plain_fp64": round(value / pl_value, 3),
             "rays_per_s": round(n * world * K / (t_fwd / 1e3), 1),
@@ -409,7 +421,9 @@ def run_ours(args):
             "e2e": {"value": round(e2e_value, 4), "unit": UNIT,
                     "h2d_bytes_per_step": int(2 * n * 3 * 8),
                     "d2h_bytes_per_step": int(n * nout * 8)},
-            "gpu_launches": 2 * K,
+            # per timed forward step: k_ray_keys, k_batched, k_slow (CUB's
+            # radix-sort kernels of the ray order not counted)
+            "gpu_launches": 3 * K,
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks,

@@ -50,14 +50,16 @@ extern "C" {
 #define VT_REDUCE_VOLUME 3
 
 /* ---- walk kernels ------------------------------------------------------ */
-#define VT_KERNEL_AUTO 0        /* the batched guarded-FP32 kernel              */
-#define VT_KERNEL_PLAIN_FP64 1  /* one ray per thread, full-FP64 k-NN           */
+#define VT_KERNEL_AUTO 0        /* the fastest exact kernel (BATCHED_FP64)      */
+#define VT_KERNEL_PLAIN_FP64 1  /* one ray per thread in the caller's order,    */
+                                /* full-FP64 k-NN from the root                 */
 #define VT_KERNEL_BATCHED 2     /* persistent queue, one warp per ray,          */
                                 /* warp-cooperative guarded-FP32 k-NN           */
-#define VT_KERNEL_BATCHED_FP64 3 /* persistent queue, one ray per thread,       */
-                                 /* bounded FP64 k-NN                           */
-#define VT_KERNEL_THREAD_FP32 4 /* persistent queue, one ray per thread,        */
-                                /* leaf-directed guarded-FP32 k-NN              */
+#define VT_KERNEL_BATCHED_FP64 3 /* persistent queue, one ray per thread, rays  */
+                                 /* in a coherent (sorted) order, bounded FP64  */
+                                 /* k-NN                                        */
+#define VT_KERNEL_THREAD_FP32 4 /* as BATCHED_FP64 with the leaf-directed       */
+                                /* guarded-FP32 k-NN                            */
 
 /* ---- tunable parameters (vt_cloud_set_param) --------------------------- */
 #define VT_PARAM_MAX_ITERATIONS 1 /* src/ray.cpp:10, default 100000           */

@@ -247,3 +247,28 @@ def test_neighbourhood_cache_is_exact(clustered):
     assert pc.last_stats["cache_hits"] == 0
     np.testing.assert_array_equal(on, off)
     np.testing.assert_array_equal(on, ot.project(S, E))
+
+
+def test_neighbourhood_cache_random_rays_and_segments(clustered):
+    """Cache on/off agree bit for bit on arbitrary directions (rays through
+    the dense core and across the whole box) and on the per-segment output."""
+    from vortrace_b200 import _lib as L
+    w, pc, (lp, ot) = clustered
+    rng = np.random.default_rng(11)
+    S = np.vstack([rng.uniform(0.0, 100.0, (1536, 3)), 50.0 + rng.normal(0.0, 3.0, (512, 3))])
+    E = np.vstack([rng.uniform(0.0, 100.0, (1536, 3)), 50.0 + rng.normal(0.0, 3.0, (512, 3))])
+    pc.kernel = "batched"
+    pc._cloud.set_param(L.PARAM_CACHE, 1)
+    try:
+        on = pc.projection(S, E)
+        hits = pc.last_stats["cache_hits"]
+        seg_on = pc.traced_projection(S[:256], E[:256], flatten=True)
+    finally:
+        pc._cloud.set_param(L.PARAM_CACHE, 0)
+    assert hits > 0
+    off = pc.projection(S, E)
+    np.testing.assert_array_equal(on, off)
+    seg_off = pc.traced_projection(S[:256], E[:256], flatten=True)
+    for a, b in zip(seg_on, seg_off):
+        np.testing.assert_array_equal(np.asarray(a), np.asarray(b))
+    np.testing.assert_array_equal(on, ot.project(S, E))

@@ -80,7 +80,7 @@ int vt::check_projectable(const vt_cloud* cl, int mode) {
 }
 
 static int resolve_kernel(int kernel) {
-  if (kernel == VT_KERNEL_AUTO) return VT_KERNEL_BATCHED;
+  if (kernel == VT_KERNEL_AUTO) return VT_KERNEL_BATCHED_FP64;
   return kernel;
 }
 
@@ -553,7 +553,7 @@ static int adjoint_locked(vt_cloud* cl, const double* d_starts, const double* d_
   io.gout = d_gout;
   io.fwd = d_out;
   io.grad = d_grad;
-  return vt::run_walk(cl, io, vt::kOutAdj, mode, VT_KERNEL_BATCHED, st, nullptr);
+  return vt::run_walk(cl, io, vt::kOutAdj, mode, resolve_kernel(VT_KERNEL_AUTO), st, nullptr);
 }
 
 int vt_project_adjoint_device(vt_cloud* cl, const double* d_starts, const double* d_ends,

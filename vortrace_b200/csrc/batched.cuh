@@ -2,10 +2,11 @@
 //
 // Same walk as walk_ray() (src/ray.cpp:187-430) restructured for SIMD
 // efficiency:
-//   * persistent grid (a multiple of the SM count); every lane owns one ray
-//     and takes a new one from a global atomic queue as soon as its ray is
-//     done (warp-aggregated atomicAdd), so long and short rays mix freely and
-//     many projections / arbitrary rays go through one launch;
+//   * persistent grid (a multiple of the SM count); every lane owns one ray;
+//     a warp takes the next 32 rays of the coherent ray order (io.order, see
+//     sort_rays) from a global atomic queue once all its lanes are done, so
+//     the 32 rays of a warp are spatial neighbours whose searches visit the
+//     same nodes, and many projections / arbitrary rays share one launch;
 //   * one loop trip = one walk iteration per lane, so all lanes issue the
 //     same k-NN search code;
 //   * the split-point query is a *bounded* 3-NN: the two cells c and n whose
@@ -19,9 +20,10 @@
 //     arithmetic); every passing point is re-checked with its FP64 distance
 //     in the reference's operation order, so results are exact;
 //   * the top tree levels live in shared memory;
-//   * rare paths (parallel bisector fallback, Case 1a, 100-NN expansion, a
-//     pending-point stack deeper than the in-register one) hand the ray to
-//     k_slow with the number of segments already emitted.
+//   * rare paths (parallel bisector fallback, Case 1a, 100-NN expansion) run
+//     inline in non-inlined functions; a pending-point stack deeper than the
+//     in-register one hands the ray to k_slow with the number of segments
+//     already emitted.
 #pragma once
 
 namespace vt {
@@ -29,7 +31,7 @@ namespace vt {
 constexpr int kBatchStack = 32;
 // resident blocks per SM the batched kernel is compiled for (register cap)
 #ifndef VT_BATCHED_MINB
-#define VT_BATCHED_MINB 4
+#define VT_BATCHED_MINB 5
 #endif
 
 // ---- node fetch (shared memory for the top levels) ----------------------
@@ -399,7 +401,13 @@ __device__ __forceinline__ bool knn3_decision_valid(const KnnList<3>& r, double 
   return dsub(R, r.r2[0]) >= kTol && dadd(r.r2[0], kTol) < R;
 }
 
-// Bound on |f - d| for points with d < R (see knn3_guarded).
+// G(R) bounds |f - d| for every point with d < R, where f is the FP32
+// distance between the FP32 images of q and p (frame origin subtracted,
+// each coordinate within e of the exact offset) and d the FP64 metric:
+// X = 3.5 e sqrt(R) + 3 e^2 bounds the change of the squared distance from
+// the coordinate errors, 6u (R + X) the FP32 rounding of the three
+// subtractions, three squares and two additions (u = 2^-24), 1e-15 R the
+// FP64 rounding of d, and the factor 1.02 leaves slack.
 __device__ __forceinline__ double guard_band(double R, double e) {
   const double u = 5.9604644775390625e-08;  // 2^-24
   const double sr = sqrt(R);
@@ -500,7 +508,10 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
 
   for (;;) {
     // ---- refill idle lanes from the work queue
-    const bool want = (phase == 0) && !exhausted;
+    // a warp takes 32 consecutive rays (of the coherent order) once all its
+    // lanes are idle: neighbouring rays visit the same tree nodes, so the
+    // lanes' searches stay convergent and share cache lines
+    const bool want = __all_sync(FULL, phase == 0) && !exhausted;
     const unsigned need = __ballot_sync(FULL, want);
     if (need) {
       const int leader = __ffs(need) - 1;
@@ -508,8 +519,9 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
       if (lane == leader) base = atomicAdd(&io.stats->next_ray, (unsigned long long)__popc(need));
       base = __shfl_sync(FULL, base, leader);
       if (want) {
-        const int64_t r = (int64_t)base + __popc(need & ((1u << lane) - 1));
-        if (r < io.nrays) {
+        const int64_t i = (int64_t)base + __popc(need & ((1u << lane) - 1));
+        if (i < io.nrays) {
+          const int64_t r = io.order ? (int64_t)io.order[i] : i;
           ray = r;
           ray_init(g, io.starts + 3 * r, io.ends + 3 * r);
           if (!ray_finite(g)) {

@@ -95,6 +95,22 @@ __device__ __forceinline__ void leaf_range(const DevCloud& c, int64_t leaf, int6
   b = ((leaf + 1) * c.n) >> c.depth;
 }
 
+// FP32 squared distance from q to the box [lo, hi] (0 inside) and to a
+// point, with the same rounding steps: for every FP32 point p inside the
+// box each per-axis gap is at most |q - p| (FP32 subtraction is monotone),
+// so box_dist32 <= pt_dist32 for all points of the box.
+__device__ __forceinline__ float box_dist32(float q0, float q1, float q2, float4 lo, float4 hi) {
+  const float a = q0 < lo.x ? __fsub_rn(lo.x, q0) : (q0 > hi.x ? __fsub_rn(q0, hi.x) : 0.f);
+  const float b = q1 < lo.y ? __fsub_rn(lo.y, q1) : (q1 > hi.y ? __fsub_rn(q1, hi.y) : 0.f);
+  const float c = q2 < lo.z ? __fsub_rn(lo.z, q2) : (q2 > hi.z ? __fsub_rn(q2, hi.z) : 0.f);
+  return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
+}
+
+__device__ __forceinline__ float pt_dist32(float q0, float q1, float q2, float4 p) {
+  const float a = __fsub_rn(q0, p.x), b = __fsub_rn(q1, p.y), c = __fsub_rn(q2, p.z);
+  return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
+}
+
 // Per-launch counters (atomically accumulated, warp-aggregated).
 struct DevStats {
   unsigned long long rays;

@@ -123,6 +123,7 @@ struct vt_cloud {
   vt::DevBuf<double> ws_stack_s;
   vt::DevBuf<vt::DevStats> ws_stats;
   vt::DevBuf<uint8_t> ws_tmp;
+  vt::DevBuf<uint8_t> ws_order;  // ray sort keys, order and CUB scratch
 };
 
 namespace vt {

@@ -504,8 +504,90 @@ static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int ker
 }
 
 // Walk launch with the handle's (grow-only) workspace as scratch.
+// ------------------------------------------------------- ray ordering
+// The batched kernels walk the rays in a coherent order: sorted by a 64-bit
+// key of the quantized direction (5 bits per component, bits 48-62) and the
+// Morton code of the ray's midpoint in the cloud's box (16 bits per axis,
+// bits 0-47).  Parallel rays of a projection grid then run as compact 2D
+// tiles, so the 32 rays of a warp cross the same cells.  Non-finite rays
+// sort last.  Results are written at each ray's own index.
+__device__ __forceinline__ unsigned long long spread3(unsigned v) {
+  unsigned long long x = v & 0xffffu;
+  x = (x | (x << 16)) & 0x0000ff0000ffULL;
+  x = (x | (x << 8)) & 0x00f00f00f00fULL;
+  x = (x | (x << 4)) & 0x0c30c30c30c3ULL;
+  x = (x | (x << 2)) & 0x249249249249ULL;
+  return x;
+}
+
+__global__ void k_ray_keys(const double* __restrict__ S, const double* __restrict__ E,
+                           int64_t n, DevCloud c, unsigned long long* keys, int32_t* idx) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s[3], e[3], d[3];
+  bool ok = true;
+  double len2 = 0.0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    s[j] = S[3 * i + j];
+    e[j] = E[3 * i + j];
+    d[j] = e[j] - s[j];
+    len2 += d[j] * d[j];
+    ok = ok && isfinite(s[j]) && isfinite(e[j]);
+  }
+  unsigned long long key = ~0ULL;
+  if (ok) {
+    const double inv = len2 > 0.0 ? 1.0 / sqrt(len2) : 0.0;
+    unsigned long long dq = 0, mc = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double u = (d[j] * inv + 1.0) * 15.5;
+      dq = (dq << 5) | (unsigned long long)(u < 0.0 ? 0 : (u > 31.0 ? 31 : (int)u));
+      const double ext = c.bbhi[j] - c.bblo[j];
+      double m = ext > 0.0 ? ((0.5 * (s[j] + e[j]) - c.bblo[j]) / ext) * 65535.0 : 0.0;
+      m = m < 0.0 ? 0.0 : (m > 65535.0 ? 65535.0 : m);
+      mc |= spread3((unsigned)m) << j;
+    }
+    key = (dq << 48) | mc;
+  }
+  keys[i] = key;
+  idx[i] = (int32_t)i;
+}
+
+// Fill io.order (workspace) with the coherent ray order.
+static int sort_rays(vt_cloud* cl, WalkIO& io, cudaStream_t st) {
+  const int64_t n = io.nrays;
+  io.order = nullptr;
+  if (n < 64 || n > (int64_t)0x7fffffff) return VT_OK;  // identity order
+  size_t cub_bytes = 0;
+  VT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (unsigned long long*)nullptr,
+                                          (unsigned long long*)nullptr, (int32_t*)nullptr,
+                                          (int32_t*)nullptr, (int)n, 0, 63, st));
+  const size_t kb = ((size_t)n * 8 + 255) & ~(size_t)255;
+  const size_t ib = ((size_t)n * 4 + 255) & ~(size_t)255;
+  if (cl->ws_order.reserve(2 * kb + 2 * ib + cub_bytes)) return VT_ERR_NOMEM;
+  uint8_t* base = cl->ws_order.p;
+  auto* k0 = reinterpret_cast<unsigned long long*>(base);
+  auto* k1 = reinterpret_cast<unsigned long long*>(base + kb);
+  auto* i0 = reinterpret_cast<int32_t*>(base + 2 * kb);
+  auto* i1 = reinterpret_cast<int32_t*>(base + 2 * kb + ib);
+  void* tmp = base + 2 * kb + 2 * ib;
+  const int B = 256;
+  k_ray_keys<<<(unsigned)((n + B - 1) / B), B, 0, st>>>(io.starts, io.ends, n, cl->view, k0, i0);
+  VT_CUDA(cudaGetLastError());
+  VT_CUDA(cub::DeviceRadixSort::SortPairs(tmp, cub_bytes, k0, k1, i0, i1, (int)n, 0, 63, st));
+  io.order = i1;
+  return VT_OK;
+}
+
 int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaStream_t st,
              vt_stats* stats) {
+  if (kernel != VT_KERNEL_PLAIN_FP64) {
+    const int rc = sort_rays(cl, io, st);
+    if (rc) return rc;
+  } else {
+    io.order = nullptr;  // the plain kernel keeps the caller's order
+  }
   const int slow_threads = 1024;
   if (cl->ws_stats.reserve(1)) return VT_ERR_NOMEM;
   if (cl->ws_slow.reserve(io.nrays > 0 ? io.nrays : 1)) return VT_ERR_NOMEM;

@@ -39,6 +39,7 @@ struct WalkIO {
   int64_t max_iter;
   int local_cap;         // in-register stack entries per ray
   int cache_mode;        // batched kernel: 1 = neighbourhood cache on
+  const int32_t* order;  // batched kernels: ray visiting order (NULL: 0..nrays-1)
   WalkDiag* diag;
 };
 

@@ -39,24 +39,19 @@ constexpr int kWWalkStack = 64;     // per-warp pending ray points
 #define VT_WARP_MINB 4
 #endif
 
-__device__ __forceinline__ float box_dist32(float q0, float q1, float q2, float4 lo, float4 hi) {
-  const float a = q0 < lo.x ? __fsub_rn(lo.x, q0) : (q0 > hi.x ? __fsub_rn(q0, hi.x) : 0.f);
-  const float b = q1 < lo.y ? __fsub_rn(lo.y, q1) : (q1 > hi.y ? __fsub_rn(q1, hi.y) : 0.f);
-  const float c = q2 < lo.z ? __fsub_rn(lo.z, q2) : (q2 > hi.z ? __fsub_rn(q2, hi.z) : 0.f);
-  return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
-}
-
-__device__ __forceinline__ float pt_dist32(float q0, float q1, float q2, float4 p) {
-  const float a = __fsub_rn(q0, p.x), b = __fsub_rn(q1, p.y), c = __fsub_rn(q2, p.z);
-  return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
-}
-
 __device__ __forceinline__ int depth_of(int v) { return 31 - __clz(v + 1); }
+
+// FP32 acceptance threshold for FP64 threshold T: every point with d < T
+// has FP32 distance f < T + G(T) (guard_band), rounded up.
+__device__ __forceinline__ float thr32_of(double T, double qe) {
+  return __double2float_ru(dadd(T, guard_band(T, qe)));
+}
 
 struct WarpQuery {
   double x, y, z;     // FP64 query
   float q0, q1, q2;   // FP32 frame
-  double bound, G;    // accept d < bound; FP32 guard band
+  double bound, G;    // accept d < bound; FP32 guard band at the bound
+  double qe;          // FP32 coordinate error of this ray's queries
   int cid, nid;       // cells with known distances (or -1)
   double dc, dn;
 };
@@ -120,7 +115,7 @@ __device__ __forceinline__ void warp_leaves(const DevCloud& c, const int lane,
       if (dj < thr64) {
         L.insert(dj, pj);
         thr64 = fmin(Q.bound, L.worst());
-        thr32 = __double2float_ru(dadd(thr64, Q.G));
+        thr32 = thr32_of(thr64, Q.qe);
       }
     }
   }
@@ -130,21 +125,29 @@ __device__ __forceinline__ void warp_leaves(const DevCloud& c, const int lane,
 // results already (then `skip_leaf`, the leaf they came from, is skipped).
 // Returns false if the per-warp stack overflowed (the result is then not
 // trustworthy and the caller re-resolves the query).
+// `start` >= 0 restricts the search to the subtree of that internal node
+// (whose own box the caller has tested); -1 searches the whole tree.
 template <int K>
 __device__ __forceinline__ bool warp_knn(const DevCloud& c, const int lane, const WarpQuery& Q,
                          const int64_t skip_leaf, KnnList<K>& L, int* s_node, float* s_mind,
-                         unsigned& nver, unsigned& nsteps) {
+                         unsigned& nver, unsigned& nsteps, const int64_t start = -1) {
   const int D = c.depth;
   const int64_t ninternal = c.nleaves - 1;
   double thr64 = fmin(Q.bound, L.worst());
-  float thr32 = __double2float_ru(dadd(thr64, Q.G));
+  float thr32 = thr32_of(thr64, Q.qe);
   int sp = 0;
   bool overflow = false;
   // group being tested: nodes [gfirst, gfirst + gm), leaves if gleaves
   int64_t gfirst;
   int gm;
   bool gleaves;
-  if (D == 0) {
+  if (start >= 0) {
+    const int k = 63 - __clzll(start + 1);
+    const int s = min(5, D - k);
+    gfirst = ((start + 1) << s) - 1;
+    gm = 1 << s;
+    gleaves = (k + s == D);
+  } else if (D == 0) {
     gfirst = 0;
     gm = 1;
     gleaves = true;
@@ -263,28 +266,36 @@ __device__ __forceinline__ void warp_query_setup(WarpQuery& Q, const DevCloud& c
   Q.q2 = __double2float_rn(dsub(z, c.origin[2]));
 }
 
-// ------------------------------------------------- capsule cache
+// ------------------------------------------------- tube cache
 // Consecutive split points of a ray lie on the ray and move forward (a
 // query's s is never below the walk's current s), so one gather of the
 // points around a stretch of the ray serves many queries.  A warp keeps a
 // "capsule" of points:
 //   every point p whose axial parameter t = (p - P_a).dir lies in [0, L]
 //   and whose distance from the ray's line is < rho is in the cache,
-// with P_a = start + s_a dir.  A split query at parameter s with bound R is
-// answered from the cache when r = sqrt(R)(1 + 1e-12) + eps satisfies
-// r <= rho and s_a <= s - r and s + r <= s_a + L: every p with
-// d64(q, p) < R has |t(p) - (s - s_a)| <= |p - q| < r and a distance from
+// with P_a = start + s_a dir.  A split query at parameter s is answered
+// from the cache when, after the scan, the final threshold
+// T = min(bound, 3rd best distance) gives r = sqrt(T)(1 + 1e-12) + eps
+// with r <= rho and s_a <= s - r and s + r <= s_a + L: every p with
+// d64(q, p) <= T has |t(p) - (s - s_a)| <= |p - q| < r and a distance from
 // the line below r <= rho, so it is cached, and the bounded 3-NN over the
 // cache is the same exact set as over the tree.  The gather's membership
 // test runs in FP64 on the FP64 points; eps covers FP64 rounding.
+//
+// The cache holds up to kCache points in gather (tree) order, split into
+// chunks of 32 with a tight FP32 box per chunk; a scan tests the chunk
+// boxes (one per lane), then visits the surviving chunks nearest first.
 #ifndef VT_WARP_CACHE
-#define VT_WARP_CACHE 64
+#define VT_WARP_CACHE 256
 #endif
 constexpr int kCache = VT_WARP_CACHE;  // points per warp
+constexpr int kChunks = kCache / 32;
+static_assert(kCache % 32 == 0 && kChunks <= 32, "cache is 1..32 chunks of 32 points");
 
 struct Capsule {
   double sa, L, rho;  // start parameter, guaranteed length and radius
-  int count;
+  int count;          // cached points
+  int total;          // points found in the requested capsule (>= count)
 };
 
 __device__ __forceinline__ bool capsule_covers(const Capsule& K, double s, double R,
@@ -294,18 +305,21 @@ __device__ __forceinline__ bool capsule_covers(const Capsule& K, double s, doubl
   return r <= K.rho && t - r >= 0.0 && t + r <= K.L;
 }
 
-// Does the segment P0 + t d, t in [t0, t1], come within w (per axis) of the
-// box [lo, hi]?  A necessary condition for any point of the box to lie
-// within distance w of the segment.
-__device__ __forceinline__ bool seg_near_box(const double P0[3], const double d[3],
-                                             const double invd[3], double t0, double t1,
-                                             float4 lo, float4 hi, double w) {
+// Entry parameter of the segment P0 + t d, t in [t0, t1], into the box
+// [lo, hi] inflated by w per axis, or +inf if it misses.  A point of the box
+// within distance w of the line has its foot on the line inside the
+// inflated box, so its axial parameter is at least the returned value (up
+// to rounding); missing the inflated box means no point of the box lies
+// within w of the segment.
+__device__ __forceinline__ double seg_box_entry(const double P0[3], const double d[3],
+                                                const double invd[3], double t0, double t1,
+                                                float4 lo, float4 hi, double w) {
   const double l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z};
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     const double l = l3[j] - w - P0[j], h = h3[j] + w - P0[j];
     if (d[j] == 0.0) {
-      if (l > 0.0 || h < 0.0) return false;
+      if (l > 0.0 || h < 0.0) return pinf();
     } else {
       double a = l * invd[j], b = h * invd[j];
       if (a > b) {
@@ -317,15 +331,31 @@ __device__ __forceinline__ bool seg_near_box(const double P0[3], const double d[
       t1 = fmin(t1, b);
     }
   }
-  return t0 <= t1 + 1e-9;
+  return t0 <= t1 + 1e-9 ? t0 : pinf();
 }
 
-// Gather the capsule (start parameter sa, length L, radius rho) of ray g.
+// float <-> int keys with the same order (finite values), for integer
+// warp reductions of FP32 coordinates
+__device__ __forceinline__ int ord_key(float f) {
+  const int k = __float_as_int(f);
+  return k >= 0 ? k : k ^ 0x7fffffff;
+}
+__device__ __forceinline__ float ord_val(int k) {
+  return __int_as_float(k >= 0 ? k : k ^ 0x7fffffff);
+}
+
+// Gather the capsule (start parameter sa, length L, radius rho) of ray g
+// into `cache` and build the chunk boxes.  The traversal continues into the
+// subtree the segment enters first; once the cache is full, the smallest
+// axial parameter of a dropped point (tdrop) shortens the capsule to
+// L' = tdrop - 2 eps, and subtrees entered beyond tdrop + eps are pruned (all
+// their capsule points lie beyond L'), which bounds the work of a gather.
 __device__ __forceinline__ Capsule warp_gather_capsule(const DevCloud& c, const int lane,
                                                        const RayGeom& g, double sa, double L,
                                                        double rho, double eps, float4* cache,
-                                                       int* s_node, unsigned& nver,
-                                                       unsigned& nsteps) {
+                                                       float4* cblo, float4* cbhi,
+                                                       int* s_node, float* s_key,
+                                                       unsigned& nver, unsigned& nsteps) {
   const int D = c.depth;
   const int64_t ninternal = c.nleaves - 1;
   double Pa[3], P0[3], invd[3];
@@ -339,7 +369,7 @@ __device__ __forceinline__ Capsule warp_gather_capsule(const DevCloud& c, const 
   const double wbox = rho + (double)c.coord_err + eps;
   const double t_lo = -eps, t_hi = L + eps;
   const double rho2_in = rho * rho * (1.0 + 1e-12) + eps * eps;
-  double tdrop = pinf();
+  double tdrop = pinf();  // warp-uniform
   int count = 0;
   int sp = 0;
   bool lost = false;
@@ -359,10 +389,11 @@ __device__ __forceinline__ Capsule warp_gather_capsule(const DevCloud& c, const 
   for (;;) {
     ++nsteps;
     const int64_t node = gfirst + lane;
-    bool surv = false;
+    double te = pinf();
     if (lane < gm)
-      surv = seg_near_box(P0, g.d, invd, t_lo, t_hi, __ldg(&c.boxlo[node]),
-                          __ldg(&c.boxhi[node]), wbox);
+      te = seg_box_entry(P0, g.d, invd, t_lo, t_hi, __ldg(&c.boxlo[node]),
+                         __ldg(&c.boxhi[node]), wbox);
+    const bool surv = te <= tdrop + eps;
     const unsigned mask = __ballot_sync(kFull, surv);
     bool next = false;
     int v = 0;
@@ -382,6 +413,7 @@ __device__ __forceinline__ Capsule warp_gather_capsule(const DevCloud& c, const 
           if (lane >= o) incl += t;
         }
         const int total = __shfl_sync(kFull, incl, 31);
+        double tmin_drop = pinf();
         for (int base = 0; base < total; base += 32) {
           const int kk = base + lane;
           int lo = 0, hi = 31;
@@ -412,29 +444,50 @@ __device__ __forceinline__ Capsule warp_gather_capsule(const DevCloud& c, const 
               P32.w = __int_as_float((int)p);
               cache[pos] = P32;
             } else {
-              tdrop = fmin(tdrop, tp);
+              tmin_drop = fmin(tmin_drop, tp);
             }
           }
           count += __popc(im);
         }
+        if (count > kCache) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1)
+            tmin_drop = fmin(tmin_drop, __shfl_xor_sync(kFull, tmin_drop, o));
+          tdrop = fmin(tdrop, tmin_drop);
+        }
       }
     } else if (mask) {
-      const unsigned rest = mask & (mask - 1u);  // first survivor continues
+      // continue into the survivor entered first, remember the others
+      const int key = surv ? ord_key(__double2float_rd(te)) : 0x7fffffff;
+      const int kmin = __reduce_min_sync(kFull, key);
+      const int w = __ffs(__ballot_sync(kFull, surv && key == kmin)) - 1;
+      const unsigned rest = mask & ~(1u << w);
       const int cnt = __popc(rest);
       if (sp + cnt > kWSearchStack) {
         lost = true;  // subtrees not remembered: no guarantee
       } else {
-        if ((rest >> lane) & 1u) s_node[sp + __popc(rest & ((1u << lane) - 1u))] = (int)node;
+        if ((rest >> lane) & 1u) {
+          const int e = sp + __popc(rest & ((1u << lane) - 1u));
+          s_node[e] = (int)node;
+          s_key[e] = __double2float_rd(te);
+        }
         sp += cnt;
       }
       __syncwarp();
-      v = (int)(gfirst + __ffs(mask) - 1);
+      v = (int)(gfirst + w);
       next = true;
     }
     if (!next) {
-      if (sp == 0) break;
-      v = s_node[--sp];
+      while (sp > 0) {
+        --sp;
+        if ((double)s_key[sp] <= tdrop + eps) {
+          v = s_node[sp];
+          next = true;
+          break;
+        }
+      }
       __syncwarp();
+      if (!next) break;
     }
     const int k = depth_of(v);
     const int s = min(5, D - k);
@@ -442,29 +495,56 @@ __device__ __forceinline__ Capsule warp_gather_capsule(const DevCloud& c, const 
     gm = 1 << s;
     gleaves = (k + s == D);
   }
-  // all lanes agree on the smallest dropped parameter
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) tdrop = fmin(tdrop, __shfl_xor_sync(kFull, tdrop, o));
+  const int kept = count < kCache ? count : kCache;
+  // tight FP32 box of each chunk of 32 cached points
+  for (int k = 0; k * 32 < kept; ++k) {
+    const int idx = k * 32 + lane;
+    const bool h = idx < kept;
+    float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (h) P = cache[idx];
+    const int x0 = __reduce_min_sync(kFull, h ? ord_key(P.x) : 0x7fffffff);
+    const int y0 = __reduce_min_sync(kFull, h ? ord_key(P.y) : 0x7fffffff);
+    const int z0 = __reduce_min_sync(kFull, h ? ord_key(P.z) : 0x7fffffff);
+    const int x1 = __reduce_max_sync(kFull, h ? ord_key(P.x) : (int)0x80000000);
+    const int y1 = __reduce_max_sync(kFull, h ? ord_key(P.y) : (int)0x80000000);
+    const int z1 = __reduce_max_sync(kFull, h ? ord_key(P.z) : (int)0x80000000);
+    if (lane == 0) {
+      cblo[k] = make_float4(ord_val(x0), ord_val(y0), ord_val(z0), 0.f);
+      cbhi[k] = make_float4(ord_val(x1), ord_val(y1), ord_val(z1), 0.f);
+    }
+  }
   __syncwarp();
   Capsule K;
   K.sa = sa;
   K.rho = rho;
-  K.count = count < kCache ? count : kCache;
+  K.count = kept;
+  K.total = count;
   K.L = lost ? -1.0 : fmin(L, tdrop - 2.0 * eps);
   return K;
 }
 
-// Bounded 3-NN over the cached points (same acceptance rule as warp_knn).
+// Bounded 3-NN over the cached points (same acceptance rule as warp_knn):
+// chunk boxes first, then the surviving chunks nearest first.  The FP32
+// guard band shrinks with the threshold: guard_band(T, qe) bounds the FP32
+// error of every point with d < T.
 __device__ __forceinline__ void warp_scan_cache(const DevCloud& c, const int lane,
-                                                const WarpQuery& Q, const float4* cache,
-                                                const int count, KnnList<3>& L,
-                                                unsigned& nver) {
+                                                const WarpQuery& Q, const double qe,
+                                                const float4* cache, const float4* cblo,
+                                                const float4* cbhi, const int count,
+                                                KnnList<3>& L, unsigned& nver) {
   L.clear();
   double thr64 = Q.bound;
-  const float thr32 = __double2float_ru(dadd(thr64, Q.G));
-#pragma unroll
-  for (int j = 0; j < kCache / 32; ++j) {
-    const int idx = j * 32 + lane;
+  float thr32 = __double2float_ru(dadd(thr64, Q.G));
+  const int nch = (count + 31) >> 5;
+  float bd = __int_as_float(0x7f800000);
+  if (lane < nch) bd = box_dist32(Q.q0, Q.q1, Q.q2, cblo[lane], cbhi[lane]);
+  unsigned m = __ballot_sync(kFull, lane < nch && bd < thr32);
+  while (m) {
+    const unsigned key = ((m >> lane) & 1u) ? __float_as_uint(bd) : 0xffffffffu;
+    const unsigned kmin = __reduce_min_sync(kFull, key);
+    const int k = __ffs(__ballot_sync(kFull, key == kmin)) - 1;
+    m &= ~(1u << k);
+    const int idx = k * 32 + lane;
     bool cand = false;
     int p = -1;
     if (idx < count) {
@@ -473,26 +553,31 @@ __device__ __forceinline__ void warp_scan_cache(const DevCloud& c, const int lan
       cand = pt_dist32(Q.q0, Q.q1, Q.q2, P) < thr32;
     }
     unsigned cm = __ballot_sync(kFull, cand);
-    if (!cm) continue;
-    double d = 0.0;
-    if (cand) {
-      if (p == Q.cid) d = Q.dc;
-      else if (p == Q.nid) d = Q.dn;
-      else {
-        d = metric(Q.x, Q.y, Q.z, ldg_pt(&c.pts[p]));
-        ++nver;
+    if (cm) {
+      double d = 0.0;
+      if (cand) {
+        if (p == Q.cid) d = Q.dc;
+        else if (p == Q.nid) d = Q.dn;
+        else {
+          d = metric(Q.x, Q.y, Q.z, ldg_pt(&c.pts[p]));
+          ++nver;
+        }
       }
-    }
-    while (cm) {
-      const int jj = __ffs(cm) - 1;
-      cm &= cm - 1;
-      const double dj = __shfl_sync(kFull, d, jj);
-      const int pj = __shfl_sync(kFull, p, jj);
-      if (dj < thr64) {
-        L.insert(dj, pj);
-        thr64 = fmin(Q.bound, L.worst());
+      bool changed = false;
+      while (cm) {
+        const int jj = __ffs(cm) - 1;
+        cm &= cm - 1;
+        const double dj = __shfl_sync(kFull, d, jj);
+        const int pj = __shfl_sync(kFull, p, jj);
+        if (dj < thr64) {
+          L.insert(dj, pj);
+          thr64 = fmin(Q.bound, L.worst());
+          changed = true;
+        }
       }
+      if (changed) thr32 = __double2float_ru(dadd(thr64, guard_band(thr64, qe)));
     }
+    m &= __ballot_sync(kFull, bd < thr32);
   }
 }
 
@@ -575,6 +660,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
   __shared__ int w_id_all[kWarpsPerBlock][kWWalkStack];
   __shared__ double w_s_all[kWarpsPerBlock][kWWalkStack];
   __shared__ float4 cache_all[kWarpsPerBlock][kCache];
+  __shared__ float4 cblo_all[kWarpsPerBlock][kChunks];
+  __shared__ float4 cbhi_all[kWarpsPerBlock][kChunks];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   int* s_node = s_node_all[wib];
@@ -582,8 +669,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
   int* w_id = w_id_all[wib];
   double* w_s = w_s_all[wib];
   float4* cache = cache_all[wib];
+  float4* cblo = cblo_all[wib];
+  float4* cbhi = cbhi_all[wib];
   const double cerr = (double)c.coord_err;
-  double cap_lambda = 12.0;  // capsule length / radius, adapted per warp
+  // capsule radius / local 3-NN radius, and length / radius (adapted per
+  // warp so that a gather about fills the cache)
+  const double cap_kappa = 2.0;
+  double cap_lambda = 14.0;
   const bool use_cache = io.cache_mode != 0;
   unsigned n_rays = 0, n_cross = 0, n_q = 0, n_res = 0, n_ver = 0, n_steps = 0, max_sp = 0;
   unsigned n_refresh = 0, n_hit = 0;
@@ -593,6 +685,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
     if (lane == 0) ray = (long long)atomicAdd(&io.stats->next_ray, 1ULL);
     ray = __shfl_sync(kFull, ray, 0);
     if (ray >= io.nrays) break;
+    if (io.order) ray = io.order[ray];
     RayGeom g;
     ray_init(g, io.starts + 3 * ray, io.ends + 3 * ray);
     if (!ray_finite(g)) {
@@ -630,6 +723,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
 
     // ---- end cells: leaf on the split-plane path, then a bounded search
     WarpQuery Q;
+    Q.qe = qe;
     auto nn_end = [&](double x, double y, double z) -> int {
       warp_query_setup(Q, c, x, y, z);
       KnnList<1> r1;
@@ -676,6 +770,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
     cap.L = -1.0;
     cap.rho = 0.0;
     cap.count = 0;
+    cap.total = 0;
     // absolute FP64 slack of the capsule tests (a few ulp of the coordinates)
     const double cap_eps = 1e-12 * (qe / 6.0e-8 + g.len + 1.0);
     int rc = 0;
@@ -739,29 +834,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
         ++n_q;
         bool good;
         bool hit = false;
-        if (use_cache) {
-          const double rho = 1.5 * sqrt(Q.bound);
-          // refresh only for queries a capsule starting at the walk's current
-          // point can reach (far split points of the bisection phase are
-          // searched in the tree directly)
-          if (!capsule_covers(cap, s, Q.bound, cap_eps) &&
-              s - cur_s <= (cap_lambda - 2.2) * rho) {
-            // radius 1.5 sqrt(R), starting rho before the walk's current
-            // point (later queries never lie behind it)
-            cap = warp_gather_capsule(c, lane, g, cur_s - rho, cap_lambda * rho, rho, cap_eps,
-                                      cache, s_node, n_ver, n_steps);
-            ++n_refresh;
-            if (cap.L < cap_lambda * rho) cap_lambda = fmax(4.0, cap_lambda * 0.75);
-            else if (cap.count < kCache / 2) cap_lambda = fmin(400.0, cap_lambda * 1.25);
-          }
-          if (capsule_covers(cap, s, Q.bound, cap_eps)) {
-            warp_scan_cache(c, lane, Q, cache, cap.count, r, n_ver);
+        if (use_cache && cap.L > 0.0 && s > cap.sa && s < cap.sa + cap.L) {
+          warp_scan_cache(c, lane, Q, qe, cache, cblo, cbhi, cap.count, r, n_ver);
+          if (capsule_covers(cap, s, fmin(Q.bound, r.worst()), cap_eps)) {
             good = true;
             hit = true;
             ++n_hit;
           }
         }
-        if (!hit) good = warp_knn<3>(c, lane, Q, -1, r, s_node, s_mind, n_ver, n_steps);
+        if (!hit) {
+          r.clear();  // a scan that missed leaves partial results
+          good = warp_knn<3>(c, lane, Q, -1, r, s_node, s_mind, n_ver, n_steps);
+        }
         if (!good || !knn3_decision_valid(r, Q.bound)) {
           ++n_res;
           good = warp_knn_unbounded<3>(c, lane, Q, qe, r, s_node, s_mind, n_ver, n_steps);
@@ -783,6 +867,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
         if (r.id[0] < 0) {
           rc = kErrNonFiniteDist;
           break;
+        }
+        if (use_cache && !hit) {
+          // Re-gather around the walk's current point when this query is
+          // local (its ball would lie in the new capsule); far split points
+          // of the bisection phase do not move the capsule.
+          const double rloc = sqrt(fmin(Q.bound, r.worst()));
+          const double rho = cap_kappa * rloc;
+          const double len = cap_lambda * rho;
+          if (rho > 0.0 && s - cur_s + rloc + rho <= len) {
+            cap = warp_gather_capsule(c, lane, g, cur_s - rho, len, rho, cap_eps, cache, cblo,
+                                      cbhi, s_node, s_mind, n_ver, n_steps);
+            ++n_refresh;
+            if (cap.total > kCache)
+              cap_lambda = fmax(2.0 * cap_kappa + 2.0, cap_lambda * 0.8);
+            else if (cap.total < (kCache * 3) / 4)
+              cap_lambda = fmin(400.0, cap_lambda * fmin(2.0, (0.85 * kCache) / fmax(1.0, (double)cap.total)));
+          }
         }
         bool has_c = false, has_n = false, three_eq = true;
 #pragma unroll
