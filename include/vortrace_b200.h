@@ -50,7 +50,7 @@ extern "C" {
 #define VT_REDUCE_VOLUME 3
 
 /* ---- walk kernels ------------------------------------------------------ */
-#define VT_KERNEL_AUTO 0        /* the fastest exact kernel (BATCHED_FP64)      */
+#define VT_KERNEL_AUTO 0        /* THREAD_FP32; BATCHED below 65,536 rays       */
 #define VT_KERNEL_PLAIN_FP64 1  /* one ray per thread in the caller's order,    */
                                 /* full-FP64 k-NN from the root                 */
 #define VT_KERNEL_BATCHED 2     /* persistent queue, one warp per ray,          */
@@ -58,8 +58,8 @@ extern "C" {
 #define VT_KERNEL_BATCHED_FP64 3 /* persistent queue, one ray per thread, rays  */
                                  /* in a coherent (sorted) order, bounded FP64  */
                                  /* k-NN                                        */
-#define VT_KERNEL_THREAD_FP32 4 /* as BATCHED_FP64 with the leaf-directed       */
-                                /* guarded-FP32 k-NN                            */
+#define VT_KERNEL_THREAD_FP32 4 /* as BATCHED_FP64 with the top-down bounded    */
+                                /* guarded-FP32 k-NN (FP64 re-checks)           */
 
 /* ---- tunable parameters (vt_cloud_set_param) --------------------------- */
 #define VT_PARAM_MAX_ITERATIONS 1 /* src/ray.cpp:10, default 100000           */

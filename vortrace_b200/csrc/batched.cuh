@@ -33,6 +33,11 @@ constexpr int kBatchStack = 32;
 #ifndef VT_BATCHED_MINB
 #define VT_BATCHED_MINB 5
 #endif
+// FP32 search stack entries: 0 = (node, bound, per-axis offsets), 1 = (node,
+// bound) with the offsets restarted from zero below a popped node
+#ifndef VT_STACK_NM
+#define VT_STACK_NM 0
+#endif
 
 // ---- node fetch (shared memory for the top levels) ----------------------
 struct Fetch64 {
@@ -135,18 +140,24 @@ __device__ __forceinline__ void knn64_fetch(const DevCloud& c, const F& fetch, d
   nvisit += visits;
 }
 
-// Guarded FP32 bounded search.  Accepts points with FP64 distance d < R,
-// keeps the 3 nearest (stable insertion).  G bounds |f - d| for every point
-// with d < R, where f is the FP32 distance from pts32.  dc/dn: the known
-// FP64 distances of the cells cid/nid (no reload).
+// Guarded FP32 bounded search, top-down from the root (nanoflann's
+// searchLevel order: nearer child first, the farther one deferred on a
+// per-thread stack if its bound is below the threshold).  Accepts points
+// with FP64 distance d < R, keeps the 3 nearest (stable insertion).  G
+// (guard_band) bounds |f - d| for every point with d < R, where f is the
+// FP32 distance from pts32; a point with f < thr64 + G is re-checked with
+// its FP64 distance.  Node bounds are FP32 lower bounds of f for every
+// point of a subtree: per-axis offsets to the split planes (nodes32:
+// divlow rounded up, divhigh rounded down), summed with monotone rounding.
+// dc/dn: the known FP64 distances of the cells cid/nid (no reload).
 template <class F>
 __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, double qx,
                                              double qy, double qz, int cid, int nid, double dc,
                                              double dn, double R, double G, KnnList<3>& res,
                                              unsigned& nvisit, unsigned& nverify) {
-  const float q32[3] = {__double2float_rn(dsub(qx, c.origin[0])),
-                        __double2float_rn(dsub(qy, c.origin[1])),
-                        __double2float_rn(dsub(qz, c.origin[2]))};
+  const float q0 = __double2float_rn(dsub(qx, c.origin[0]));
+  const float q1 = __double2float_rn(dsub(qy, c.origin[1]));
+  const float q2 = __double2float_rn(dsub(qz, c.origin[2]));
   res.clear();
   double thr64 = R;
   float thr32 = __double2float_ru(dadd(thr64, G));
@@ -154,16 +165,21 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
   const int64_t ninternal = c.nleaves - 1;
   int node = 0;
   int sp = 0;
+#if VT_STACK_NM
+  int2 s_e[kMaxDepth + 2];  // (node, bound)
+  float base = 0.f;         // bound of the subtree being searched
+#else
   int s_node[kMaxDepth + 2];
   float s_off[kMaxDepth + 2][3];
   float s_mind[kMaxDepth + 2];
+#endif
   unsigned visits = 0, ver = 0;
   for (;;) {
     ++visits;
     if (node < ninternal) {
       const float2 nd = fetch(node);
       const int dim = node_dim32(nd.x);
-      const float val = q32[dim];
+      const float val = dim == 0 ? q0 : (dim == 1 ? q1 : q2);
       const int first = 2 * node + 1;
       int best, other;
       float o;
@@ -177,159 +193,16 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
         o = val > nd.x ? __fsub_rn(val, nd.x) : 0.f;  // left child: p <= lo32
       }
       const float t = __fmul_rn(o, o);
-      const float o0 = dim == 0 ? t : off[0];
-      const float o1 = dim == 1 ? t : off[1];
-      const float o2 = dim == 2 ? t : off[2];
-      const float nm = __fadd_rn(__fadd_rn(o0, o1), o2);
-      if (nm < thr32) {
-        s_node[sp] = other;
-        s_mind[sp] = nm;
-        s_off[sp][0] = o0;
-        s_off[sp][1] = o1;
-        s_off[sp][2] = o2;
-        ++sp;
-      }
-      node = best;
-      continue;
-    }
-    {
-      int64_t a, b;
-      leaf_range(c, node - ninternal, a, b);
-      for (int64_t p = a; p < b; ++p) {
-        const float4 P = __ldg(&c.pts32[p]);
-        const float d0 = __fsub_rn(q32[0], P.x), d1 = __fsub_rn(q32[1], P.y),
-                    d2 = __fsub_rn(q32[2], P.z);
-        const float f =
-            __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
-        if (f < thr32) {
-          const int pi = (int)p;
-          double d;
-          if (pi == cid) d = dc;
-          else if (pi == nid) d = dn;
-          else {
-            d = metric(qx, qy, qz, ldg_pt(&c.pts[p]));
-            ++ver;
-          }
-          if (d < thr64) {
-            res.insert(d, pi);
-            thr64 = fmin(R, res.worst());
-            thr32 = __double2float_ru(dadd(thr64, G));
-          }
-        }
-      }
-    }
-    bool found = false;
-    while (sp > 0) {
-      --sp;
-      if (s_mind[sp] < thr32) {
-        node = s_node[sp];
-        off[0] = s_off[sp][0];
-        off[1] = s_off[sp][1];
-        off[2] = s_off[sp][2];
-        found = true;
-        break;
-      }
-    }
-    if (!found) break;
-  }
-  nvisit += visits;
-  nverify += ver;
-}
-
-// Leaf-directed guarded FP32 bounded search.  The query ball B(q, sqrt(R))
-// always contains c (cid), so the search starts from c's leaf, whose index
-// is known without descending: leaf(c) = (((c+1) << depth) - 1) / n.  The
-// root-to-leaf path of that leaf is walked with independent node loads (no
-// data-dependent branching); every sibling subtree of the path whose box
-// (the conservative FP32 box implied by the path's splits) is within the
-// current threshold is pushed, the leaf is scanned, and the pushed
-// subtrees are then searched depth-first, deepest first.  Same acceptance
-// rule and FP64 re-check as knn3_guarded, so the result is the same exact
-// set; only the visiting order (and so the order of exactly tied points)
-// differs.
-template <class F>
-__device__ __forceinline__ void knn3_leafdir(const DevCloud& c, const F& fetch, double qx,
-                                             double qy, double qz, int cid, int nid, double dc,
-                                             double dn, double R, double G, KnnList<3>& res,
-                                             unsigned& nvisit, unsigned& nverify) {
-  const float q32[3] = {__double2float_rn(dsub(qx, c.origin[0])),
-                        __double2float_rn(dsub(qy, c.origin[1])),
-                        __double2float_rn(dsub(qz, c.origin[2]))};
-  res.clear();
-  double thr64 = R;
-  float thr32 = __double2float_ru(dadd(thr64, G));
-  const int D = c.depth;
-  const int64_t ninternal = c.nleaves - 1;
-  const int64_t leaf0 = ((((int64_t)cid + 1) << D) - 1) / c.n;
-  const int64_t h1 = ninternal + leaf0 + 1;  // 1-based heap index of the leaf
-  float Lb[3] = {c.bblo32[0], c.bblo32[1], c.bblo32[2]};
-  float Ub[3] = {c.bbhi32[0], c.bbhi32[1], c.bbhi32[2]};
-  int sp = 0;
-  int s_node[kMaxDepth + 2];
-  float s_off[kMaxDepth + 2][3];
-  float s_mind[kMaxDepth + 2];
-  unsigned visits = 0, ver = 0;
-  auto box_off = [](float q, float lo, float hi) -> float {
-    return q < lo ? __fsub_rn(lo, q) : (q > hi ? __fsub_rn(q, hi) : 0.f);
-  };
-  // --- the path: ancestors of the leaf, siblings within reach are pushed
-  for (int k = 0; k < D; ++k) {
-    const int a = (int)((h1 >> (D - k)) - 1);
-    const int right = (int)((h1 >> (D - k - 1)) & 1);
-    const float2 nd = fetch(a);
-    const int dim = node_dim32(nd.x);
-    float sL = Lb[dim], sU = Ub[dim];
-    if (right) {  // path -> right child (p >= hi32); sibling = left (p <= lo32)
-      sU = fminf(sU, nd.x);
-      Lb[dim] = fmaxf(Lb[dim], nd.y);
-    } else {
-      sL = fmaxf(sL, nd.y);
-      Ub[dim] = fminf(Ub[dim], nd.x);
-    }
-    // sibling box = ancestor box with [sL, sU] along `dim` (Lb/Ub of the
-    // other dims are the ancestor's: only `dim` changed at this level)
-    float o[3];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const float ob = box_off(q32[j], j == dim ? sL : Lb[j], j == dim ? sU : Ub[j]);
-      o[j] = __fmul_rn(ob, ob);
-    }
-    const float nm = __fadd_rn(__fadd_rn(o[0], o[1]), o[2]);
-    ++visits;
-    if (nm < thr32) {
-      s_node[sp] = right ? 2 * a + 1 : 2 * a + 2;
-      s_mind[sp] = nm;
-      s_off[sp][0] = o[0];
-      s_off[sp][1] = o[1];
-      s_off[sp][2] = o[2];
-      ++sp;
-    }
-  }
-  // --- scan c's leaf, then the pushed subtrees
-  int64_t node = ninternal + leaf0;
-  float off[3] = {0.f, 0.f, 0.f};
-  for (;;) {
-    ++visits;
-    if (node < ninternal) {
-      const float2 nd = fetch(node);
-      const int dim = node_dim32(nd.x);
-      const float val = q32[dim];
-      const int first = 2 * (int)node + 1;
-      int best, other;
-      float o;
-      if (__fadd_rn(__fsub_rn(val, nd.x), __fsub_rn(val, nd.y)) < 0.f) {
-        best = first;
-        other = first + 1;
-        o = nd.y > val ? __fsub_rn(nd.y, val) : 0.f;
-      } else {
-        best = first + 1;
-        other = first;
-        o = val > nd.x ? __fsub_rn(val, nd.x) : 0.f;
-      }
-      const float t = __fmul_rn(o, o);
       const float o0 = dim == 0 ? fmaxf(t, off[0]) : off[0];
       const float o1 = dim == 1 ? fmaxf(t, off[1]) : off[1];
       const float o2 = dim == 2 ? fmaxf(t, off[2]) : off[2];
+#if VT_STACK_NM
+      const float nm = fmaxf(__fadd_rn(__fadd_rn(o0, o1), o2), base);
+      if (nm < thr32) {
+        s_e[sp] = make_int2(other, __float_as_int(nm));
+        ++sp;
+      }
+#else
       const float nm = __fadd_rn(__fadd_rn(o0, o1), o2);
       if (nm < thr32) {
         s_node[sp] = other;
@@ -339,17 +212,17 @@ __device__ __forceinline__ void knn3_leafdir(const DevCloud& c, const F& fetch, 
         s_off[sp][2] = o2;
         ++sp;
       }
+#endif
       node = best;
       continue;
     }
     {
       int64_t a, b;
       leaf_range(c, node - ninternal, a, b);
-#pragma unroll 2
       for (int64_t p = a; p < b; ++p) {
         const float4 P = __ldg(&c.pts32[p]);
-        const float d0 = __fsub_rn(q32[0], P.x), d1 = __fsub_rn(q32[1], P.y),
-                    d2 = __fsub_rn(q32[2], P.z);
+        const float d0 = __fsub_rn(q0, P.x), d1 = __fsub_rn(q1, P.y),
+                    d2 = __fsub_rn(q2, P.z);
         const float f =
             __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
         if (f < thr32) {
@@ -372,6 +245,16 @@ __device__ __forceinline__ void knn3_leafdir(const DevCloud& c, const F& fetch, 
     bool found = false;
     while (sp > 0) {
       --sp;
+#if VT_STACK_NM
+      const int2 e = s_e[sp];
+      if (__int_as_float(e.y) < thr32) {
+        node = e.x;
+        base = __int_as_float(e.y);
+        off[0] = off[1] = off[2] = 0.f;
+        found = true;
+        break;
+      }
+#else
       if (s_mind[sp] < thr32) {
         node = s_node[sp];
         off[0] = s_off[sp][0];
@@ -380,6 +263,7 @@ __device__ __forceinline__ void knn3_leafdir(const DevCloud& c, const F& fetch, 
         found = true;
         break;
       }
+#endif
     }
     if (!found) break;
   }
@@ -643,7 +527,7 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
       ++n_q;
       if (G32) {
         const double G = guard_band(R, q_err);
-        knn3_leafdir(c, f32, qx, qy, qz, cur, nxt, dc, dn, R, G, r, n_visit, n_ver);
+        knn3_guarded(c, f32, qx, qy, qz, cur, nxt, dc, dn, R, G, r, n_visit, n_ver);
       } else {
         r.clear();
         knn64_fetch(c, f64, qx, qy, qz, R, r, n_visit);

@@ -101,7 +101,7 @@ struct vt_cloud {
   int stack_cap = 4096;
   int leaf_size = 8;
   int block_size = 128;
-  int smem_levels = 9;
+  int smem_levels = 5;
   int blocks_per_sm = 0;
   int local_stack = 1 << 30;  // capped to the compiled size in the kernels
   int cache_mode = 0;
