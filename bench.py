@@ -47,6 +47,11 @@ UNIT = "Mcrossings/s"
 # measured with the nanoflann restatement (oracle/measure_bx.py, 8192-ray sample).
 BX = {"clustered_2m": 3262.25, "uniform_100k": 2915.74}
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per crossing of
+# the AUTO kernel, from one ncu capture of the 512x512 case of clustered_2m
+# (profiles/k_batched_fp32_clustered_2m_npix512.md: 3.79 GB for 49,726,019
+# crossings); the full-size launch is taken to scale with its crossings.
+DRAM_BYTES_PER_CROSSING = {"clustered_2m": 76.2}
 
 
 def dist_env():
@@ -377,13 +382,8 @@ def run_ours(args):
     roof = None
     if bx and launch_ms:
         achieved = crossings * bx / (launch_ms / 1e3) / 1e9
-        traffic = None
-        tp = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tp):
-            with open(tp) as f:
-                tj = json.load(f).get(args.config)
-            if tj and tj.get("dram_bytes_per_crossing"):
-                traffic = float(tj["dram_bytes_per_crossing"]) * crossings
+        dpc = DRAM_BYTES_PER_CROSSING.get(args.config)
+        traffic = round(dpc * crossings) if dpc else None
         roof = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "peak_source": peak_src, "bytes_per_crossing": bx,
