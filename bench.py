@@ -262,6 +262,24 @@ def run_ours(args):
                                               d_out.data_ptr(), d_gout.data_ptr(),
                                               d_grad.data_ptr(), stream.cuda_stream))
 
+    # forward with a segment tape + scatter adjoint (the autograd path of
+    # 'integrate'); other reductions re-walk the rays in the adjoint
+    tape = L.Tape(lib, h)
+    taped = mode == L.REDUCE_SUM
+
+    def fwd_tape():
+        if not taped:
+            fwd(L.KERNEL_AUTO)
+            return
+        L.check(lib.vt_project_device_tape(h, tape.h, d_s.data_ptr(), d_e.data_ptr(), n, mode,
+                                           L.KERNEL_AUTO, d_out.data_ptr(),
+                                           stream.cuda_stream, C.byref(st)))
+
+    def bwd_tape():
+        L.check(lib.vt_tape_adjoint_device(h, tape.h, d_s.data_ptr(), d_e.data_ptr(), n, mode,
+                                           d_out.data_ptr(), d_gout.data_ptr(),
+                                           d_grad.data_ptr(), stream.cuda_stream))
+
     def barrier():
         torch.cuda.synchronize(dev)
         if world > 1:
@@ -318,18 +336,28 @@ def run_ours(args):
     tot_cross = reduce_sum(float(crossings))
     value = tot_cross * K / (t_fwd / 1e3) / 1e6
 
-    # --- forward + adjoint
-    for _ in range(max(1, W // 2)):
-        fwd(L.KERNEL_AUTO)
-        bwd()
+    # --- forward + adjoint (taped forward, scatter adjoint)
+    for _ in range(max(2, W // 2)):
+        fwd_tape()
+        bwd_tape()
     barrier()
-    fb_ms = timed(lambda: (fwd(L.KERNEL_AUTO), bwd()), K)
+    fb_ms = timed(lambda: (fwd_tape(), bwd_tape()), K)
     barrier()
     t_fb = reduce_max(sum(fb_ms))
     fb_value = tot_cross * K / (t_fb / 1e3) / 1e6
+    tape_entries = int(lib.vt_tape_size(tape.h))
+
+    # --- forward + adjoint that re-walks the rays (no tape)
+    kp = max(2, K // 2)
+    fwd(L.KERNEL_AUTO)
+    bwd()
+    barrier()
+    rw_ms = timed(lambda: (fwd(L.KERNEL_AUTO), bwd()), kp)
+    barrier()
+    t_rw = reduce_max(sum(rw_ms))
+    rw_value = tot_cross * kp / (t_rw / 1e3) / 1e6
 
     # --- the batched kernel with the bounded FP64 k-NN
-    kp = max(2, K // 2)
     fwd(L.KERNEL_BATCHED_FP64)
     barrier()
     f64_ms = timed(lambda: fwd(L.KERNEL_BATCHED_FP64), kp)
@@ -412,6 +440,9 @@ def run_ours(args):
                        "tree_build_ms": round(info.tree_build_ms, 2),
                        "parallelism": f"rays sharded by view, {world} rank(s)"},
             "fwd_bwd_mcrossings_per_s": round(fb_value, 4),
+            "fwd_bwd_adjoint": ("segment tape (16 B/crossing) + scatter" if taped and
+                                tape_entries > 0 else "re-walk"),
+            "fwd_bwd_rewalk_mcrossings_per_s": round(rw_value, 4),
             "kernel": "batched (VT_KERNEL_AUTO = VT_KERNEL_THREAD_FP32)",
             "bounded_fp64_mcrossings_per_s": round(f64_value, 4),
             "plain_fp64_mcrossings_per_s": round(pl_value, 4),

@@ -77,6 +77,7 @@ extern "C" {
 
 typedef struct vt_cloud vt_cloud;
 typedef struct vt_segments vt_segments;
+typedef struct vt_tape vt_tape;
 
 typedef struct {
   uint64_t npart;      /* points after filtering (PointCloud::get_npart)   */
@@ -208,6 +209,28 @@ int vt_project_adjoint(vt_cloud *cloud, const double *starts, const double *ends
 int vt_project_adjoint_device(vt_cloud *cloud, const double *d_starts, const double *d_ends,
                               uint64_t nrays, int mode, const double *d_out,
                               const double *d_grad_out, double *d_grad_fields, void *stream);
+
+/* Segment tape (no reference counterpart; the reference has no gradients).
+ * vt_project_device_tape is vt_project_device for SUM that also records, in
+ * device memory owned by the tape, one (cell, ray, ds) entry per segment --
+ * 16 bytes per crossing (3.2 GB for 2e8 crossings).  vt_tape_adjoint_device
+ * then computes the SUM adjoint as a scatter of those entries instead of a
+ * second walk.  The tape grows to the entries the last forward on it
+ * needed; a forward whose segments did not fit leaves the tape invalid, and
+ * the adjoint of an invalid or mismatched tape (other cloud, ray count or
+ * mode) re-walks the rays like vt_project_adjoint_device, so the result is
+ * the same either way.  One tape per forward whose adjoint is pending. */
+int vt_tape_create(vt_cloud *cloud, vt_tape **out);
+void vt_tape_destroy(vt_tape *tape);
+/* Entries recorded by the last forward on the tape; 0 if they did not fit. */
+uint64_t vt_tape_size(const vt_tape *tape);
+int vt_project_device_tape(vt_cloud *cloud, vt_tape *tape, const double *d_starts,
+                           const double *d_ends, uint64_t nrays, int mode, int kernel,
+                           double *d_out, void *stream, vt_stats *stats);
+int vt_tape_adjoint_device(vt_cloud *cloud, vt_tape *tape, const double *d_starts,
+                           const double *d_ends, uint64_t nrays, int mode,
+                           const double *d_out, const double *d_grad_out,
+                           double *d_grad_fields, void *stream);
 
 #ifdef __cplusplus
 }

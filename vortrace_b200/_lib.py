@@ -43,6 +43,8 @@ EXPORTS = (
     "vt_project", "vt_project_device", "vt_project_device_noalloc", "vt_project_detailed",
     "vt_segments_count",
     "vt_segments_copy", "vt_segments_free", "vt_project_adjoint", "vt_project_adjoint_device",
+    "vt_tape_create", "vt_tape_destroy", "vt_tape_size", "vt_project_device_tape",
+    "vt_tape_adjoint_device",
 )
 
 
@@ -124,12 +126,21 @@ def load(path: str | None = None):
         L.vt_segments_free.restype = None
         L.vt_project_adjoint.argtypes = [vp, dp, dp, u64, C.c_int, dp, dp, dp]
         L.vt_project_adjoint_device.argtypes = [vp, vp, vp, u64, C.c_int, vp, vp, vp, vp]
+        L.vt_tape_create.argtypes = [vp, C.POINTER(vp)]
+        L.vt_tape_destroy.argtypes = [vp]
+        L.vt_tape_destroy.restype = None
+        L.vt_tape_size.argtypes = [vp]
+        L.vt_tape_size.restype = u64
+        L.vt_project_device_tape.argtypes = [vp, vp, vp, vp, u64, C.c_int, C.c_int, vp, vp,
+                                             C.POINTER(Stats)]
+        L.vt_tape_adjoint_device.argtypes = [vp, vp, vp, vp, u64, C.c_int, vp, vp, vp, vp]
         for name in ("vt_cloud_create", "vt_cloud_build_tree", "vt_cloud_set_param",
                      "vt_cloud_set_fields", "vt_cloud_set_fields_device",
                      "vt_cloud_get_info", "vt_cloud_orig_ids", "vt_knn", "vt_project",
                      "vt_project_device", "vt_project_device_noalloc", "vt_project_detailed",
                      "vt_segments_copy",
-                     "vt_project_adjoint", "vt_project_adjoint_device", "vt_set_device"):
+                     "vt_project_adjoint", "vt_project_adjoint_device", "vt_set_device",
+                     "vt_tape_create", "vt_project_device_tape", "vt_tape_adjoint_device"):
             getattr(L, name).restype = C.c_int
         L.vt_set_warning_callback(_warn_cb)
         _lib = L
@@ -162,3 +173,20 @@ def dptr(a):
 
 def i64ptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_int64)) if a is not None else None
+
+
+class Tape:
+    """Owner of a vt_tape handle (segment tape of a taped 'integrate'
+    forward); destroyed with the object."""
+
+    def __init__(self, lib, cloud_handle):
+        self._lib = lib
+        h = C.c_void_p()
+        check(lib.vt_tape_create(cloud_handle, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            self._lib.vt_tape_destroy(h)
+            self.h = None

@@ -4,7 +4,10 @@ The reference has no gradients.  Here the forward is the walk kernel and the
 backward is the hand-written adjoint kernel (vt_project_adjoint_device):
 
 * ``'integrate'``: dL/dfield[c, f] = sum over segments of ray r in cell c of
-  dL/dimg[r, f] * ds;
+  dL/dimg[r, f] * ds.  When a gradient is needed the forward records a
+  segment tape (16 bytes per crossing, vt_project_device_tape) and the
+  backward is a scatter of it (vt_tape_adjoint_device); a tape that did not
+  fit falls back to re-walking the rays;
 * ``'volume'``: reverse-mode front-to-back compositing; the transmittance in
   front of every segment and the light behind it are recomputed by re-walking
   the ray (no per-ray segment lists are stored).
@@ -28,6 +31,18 @@ def _dev_ptr(t: torch.Tensor) -> int:
     return t.data_ptr()
 
 
+def _take_tape(pc: ProjectionCloud) -> L.Tape:
+    """A free tape of this cloud (its device buffer is reused), or a new one."""
+    pool = pc.__dict__.setdefault("_tapes", [])
+    return pool.pop() if pool else L.Tape(pc._cloud._lib, pc._cloud._h)
+
+
+def _give_back_tape(pc: ProjectionCloud, tape: L.Tape) -> None:
+    pool = pc.__dict__.setdefault("_tapes", [])
+    if not pool:  # keep one free tape per cloud; others free their memory
+        pool.append(tape)
+
+
 class _ProjectFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, fields_internal, pc: ProjectionCloud, starts, ends, mode, kernel):
@@ -41,8 +56,16 @@ class _ProjectFn(torch.autograd.Function):
         nout = 3 if mode == L.REDUCE_VOLUME else f.shape[1]
         out = torch.empty((n, nout), dtype=torch.float64, device=dev)
         st = L.Stats()
-        L.check(lib.vt_project_device(h, _dev_ptr(starts), _dev_ptr(ends), n, mode, kernel,
-                                      _dev_ptr(out), stream, C.byref(st)))
+        tape = None
+        if mode == L.REDUCE_SUM and ctx.needs_input_grad[0]:
+            tape = _take_tape(pc)
+            L.check(lib.vt_project_device_tape(h, tape.h, _dev_ptr(starts), _dev_ptr(ends), n,
+                                               mode, kernel, _dev_ptr(out), stream,
+                                               C.byref(st)))
+        else:
+            L.check(lib.vt_project_device(h, _dev_ptr(starts), _dev_ptr(ends), n, mode, kernel,
+                                          _dev_ptr(out), stream, C.byref(st)))
+        ctx.tape = tape
         pc.last_stats = st.as_dict()
         ctx.pc = pc
         ctx.mode = mode
@@ -62,9 +85,16 @@ class _ProjectFn(torch.autograd.Function):
         L.check(lib.vt_cloud_set_fields_device(h, _dev_ptr(ctx.fields), stream))
         g = gout.to(dtype=torch.float64).contiguous()
         grad = torch.zeros_like(ctx.fields)
-        L.check(lib.vt_project_adjoint_device(h, _dev_ptr(starts), _dev_ptr(ends),
-                                              starts.shape[0], ctx.mode, _dev_ptr(out),
-                                              _dev_ptr(g), _dev_ptr(grad), stream))
+        if ctx.tape is not None:
+            L.check(lib.vt_tape_adjoint_device(h, ctx.tape.h, _dev_ptr(starts), _dev_ptr(ends),
+                                               starts.shape[0], ctx.mode, _dev_ptr(out),
+                                               _dev_ptr(g), _dev_ptr(grad), stream))
+            _give_back_tape(pc, ctx.tape)
+            ctx.tape = None
+        else:
+            L.check(lib.vt_project_adjoint_device(h, _dev_ptr(starts), _dev_ptr(ends),
+                                                  starts.shape[0], ctx.mode, _dev_ptr(out),
+                                                  _dev_ptr(g), _dev_ptr(grad), stream))
         return grad, None, None, None, None, None
 
 

@@ -22,6 +22,8 @@ int run_knn(vt_cloud* cl, const double* d_q, int64_t nq, int k, int64_t* d_ids, 
             cudaStream_t st);
 int scan_offsets(vt_cloud* cl, const int64_t* d_counts, int64_t* d_offsets, int64_t n,
                  cudaStream_t st);
+int run_tape_scatter(vt_cloud* cl, const void* tape, uint64_t n, const double* d_gout,
+                     double* d_grad, cudaStream_t st);
 }  // namespace vt
 
 namespace {
@@ -578,6 +580,106 @@ int vt_project_adjoint_device(vt_cloud* cl, const double* d_starts, const double
   if (nrays == 0) return VT_OK;
   return adjoint_locked(cl, d_starts, d_ends, nrays, mode, d_out, d_grad_out, d_grad_fields,
                         pick_stream(cl, stream));
+  VT_GUARD_END
+}
+
+int vt_tape_create(vt_cloud* cl, vt_tape** out) {
+  VT_GUARD_BEGIN
+  if (!out) return set_error(VT_ERR_INVALID, "out must not be NULL");
+  *out = nullptr;
+  if (!cl) return set_error(VT_ERR_INVALID, "null cloud handle");
+  vt_tape* t = new vt_tape();
+  t->device = cl->device;
+  *out = t;
+  return VT_OK;
+  VT_GUARD_END
+}
+
+void vt_tape_destroy(vt_tape* t) {
+  if (!t) return;
+  cudaSetDevice(t->device);
+  delete t;
+}
+
+uint64_t vt_tape_size(const vt_tape* t) { return (t && t->valid) ? t->n : 0; }
+
+int vt_project_device_tape(vt_cloud* cl, vt_tape* tape, const double* d_starts,
+                           const double* d_ends, uint64_t nrays, int mode, int kernel,
+                           double* d_out, void* stream, vt_stats* stats) {
+  VT_GUARD_BEGIN
+  int rc = check_projectable(cl, mode);
+  if (rc) return rc;
+  if (!tape) return set_error(VT_ERR_INVALID, "null tape handle");
+  if (mode != VT_REDUCE_SUM) return set_error(VT_ERR_INVALID, "a tape is recorded for 'integrate' only");
+  if (nrays > (uint64_t)std::numeric_limits<int32_t>::max())
+    return set_error(VT_ERR_INVALID, "a taped projection takes at most 2^31-1 rays");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  VT_CUDA(cudaSetDevice(cl->device));
+  if (stats) memset(stats, 0, sizeof(*stats));
+  tape->valid = false;
+  tape->n = 0;
+  tape->nrays = nrays;
+  tape->nfields = cl->nfields;
+  tape->cloud = cl;
+  if (nrays == 0) {
+    tape->valid = true;
+    return VT_OK;
+  }
+  // size: the entries the last taped forward needed, else an estimate from
+  // the cloud's last walk (25% margin); a tape that overflows is invalid and
+  // its adjoint re-walks the rays
+  uint64_t need = tape->want;
+  if (cl->cross_per_ray > 0.0)
+    need = std::max<uint64_t>(need, (uint64_t)(1.25 * cl->cross_per_ray * (double)nrays) + 1024);
+  if (need > tape->cap) {
+    if ((rc = tape->buf.reserve(need * sizeof(vt::TapeEntry)))) return rc;
+    tape->cap = need;
+  }
+  if ((rc = tape->count.reserve(1))) return rc;
+  cudaStream_t st = pick_stream(cl, stream);
+  VT_CUDA(cudaMemsetAsync(tape->count.p, 0, sizeof(unsigned long long), st));
+  vt::WalkIO io{};
+  io.starts = d_starts;
+  io.ends = d_ends;
+  io.nrays = (int64_t)nrays;
+  io.nout = (int)cl->nfields;
+  io.out = d_out;
+  io.tape = reinterpret_cast<vt::TapeEntry*>(tape->buf.p);
+  io.tape_count = tape->count.p;
+  io.tape_cap = tape->cap;
+  // the warp-per-ray kernel keeps no tape: AUTO and BATCHED run one ray per thread
+  int k = resolve_kernel(kernel, nrays);
+  if (k == VT_KERNEL_BATCHED) k = VT_KERNEL_THREAD_FP32;
+  if ((rc = vt::run_walk(cl, io, vt::kOutTape, mode, k, st, stats))) return rc;
+  unsigned long long used = 0;
+  VT_CUDA(cudaMemcpyAsync(&used, tape->count.p, sizeof(used), cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  tape->want = used;
+  tape->n = used <= tape->cap ? used : 0;
+  tape->valid = used <= tape->cap;
+  return VT_OK;
+  VT_GUARD_END
+}
+
+int vt_tape_adjoint_device(vt_cloud* cl, vt_tape* tape, const double* d_starts,
+                           const double* d_ends, uint64_t nrays, int mode, const double* d_out,
+                           const double* d_grad_out, double* d_grad_fields, void* stream) {
+  VT_GUARD_BEGIN
+  int rc = check_projectable(cl, mode);
+  if (rc) return rc;
+  if (!tape) return set_error(VT_ERR_INVALID, "null tape handle");
+  if (mode != VT_REDUCE_SUM && mode != VT_REDUCE_VOLUME)
+    return set_error(VT_ERR_INVALID, "adjoint is defined for 'integrate' and 'volume' only");
+  if (mode == VT_REDUCE_VOLUME && !d_out)
+    return set_error(VT_ERR_INVALID, "the volume adjoint needs the forward output");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  VT_CUDA(cudaSetDevice(cl->device));
+  if (nrays == 0) return VT_OK;
+  cudaStream_t st = pick_stream(cl, stream);
+  if (mode == VT_REDUCE_SUM && tape->valid && tape->cloud == cl && tape->nrays == nrays &&
+      tape->nfields == cl->nfields)
+    return vt::run_tape_scatter(cl, tape->buf.p, tape->n, d_grad_out, d_grad_fields, st);
+  return adjoint_locked(cl, d_starts, d_ends, nrays, mode, d_out, d_grad_out, d_grad_fields, st);
   VT_GUARD_END
 }
 

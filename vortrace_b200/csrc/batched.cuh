@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
   st.clear();
   double q_err = 0.0;
   // sinks
-  Reducer<MODE, NF> red;
+  std::conditional_t<OUT == kOutTape, TapeReducer<MODE, NF>, Reducer<MODE, NF>> red;
   FillSink fill;
   AdjSink<MODE, NF> adj;
   // lane counters
@@ -413,7 +413,9 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
           } else {
             phase = 1;
             ++n_rays;
-            if (OUT == kOutImage || OUT == kOutCount) red.init(&c, io.out + r * io.nout);
+            if (OUT == kOutImage || OUT == kOutCount || OUT == kOutTape)
+              red.init(&c, io.out + r * io.nout);
+            if constexpr (OUT == kOutTape) red.set_tape(&io, r, 0u);
             else if (OUT == kOutFill) fill.init(&c, io, r);
             else adj.init(&c, io, r, 0u);
             double m = 0.0;
@@ -431,17 +433,17 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
 
     unsigned nseg_now = 0;
     auto nseg_of = [&]() -> unsigned {
-      if (OUT == kOutImage || OUT == kOutCount) return red.nseg;
+      if (OUT == kOutImage || OUT == kOutCount || OUT == kOutTape) return red.nseg;
       if (OUT == kOutFill) return fill.nseg;
       return adj.nseg;
     };
     auto emit = [&](int cell, double a, double b) {
-      if (OUT == kOutImage || OUT == kOutCount) red.seg(cell, a, b);
+      if (OUT == kOutImage || OUT == kOutCount || OUT == kOutTape) red.seg(cell, a, b);
       else if (OUT == kOutFill) fill.seg(cell, a, b);
       else adj.seg(cell, a, b);
     };
     auto finish_ok = [&]() {
-      if (OUT == kOutImage || OUT == kOutCount) {
+      if (OUT == kOutImage || OUT == kOutCount || OUT == kOutTape) {
         red.write(io.out + ray * io.nout);
         if (OUT == kOutCount) io.counts[ray] = red.nseg;
       }

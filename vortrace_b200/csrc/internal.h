@@ -115,6 +115,7 @@ struct vt_cloud {
   vt::DevBuf<float4> boxlo_d, boxhi_d;
   vt::DevCloud view{};
   double build_ms = 0.0;
+  double cross_per_ray = 0.0;  // crossings per ray of the last walk (tape sizing)
   // per-call workspace (grow-only)
   vt::DevBuf<double> ws_starts, ws_ends, ws_out, ws_gout, ws_grad;
   vt::DevBuf<int64_t> ws_counts;
@@ -124,6 +125,22 @@ struct vt_cloud {
   vt::DevBuf<vt::DevStats> ws_stats;
   vt::DevBuf<uint8_t> ws_tmp;
   vt::DevBuf<uint8_t> ws_order;  // ray sort keys, order and CUB scratch
+};
+
+// Segment tape of one 'integrate' forward (vt_project_device_tape): the
+// entries (cell, ray, ds) of every segment, in no particular order, so that
+// the adjoint is a scatter instead of a second walk.
+struct vt_tape {
+  int device = 0;
+  vt::DevBuf<uint8_t> buf;                 // TapeEntry[cap]
+  vt::DevBuf<unsigned long long> count;    // entries appended by the last forward
+  uint64_t cap = 0;     // entries buf holds
+  uint64_t n = 0;       // entries recorded by the last forward
+  uint64_t want = 0;    // entries the last forward needed
+  uint64_t nrays = 0;   // rays of the last forward
+  uint64_t nfields = 0;
+  const vt_cloud* cloud = nullptr;
+  bool valid = false;   // the last forward recorded every segment
 };
 
 namespace vt {

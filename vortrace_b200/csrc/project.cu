@@ -21,6 +21,7 @@
 
 #include <chrono>
 #include <cstdio>
+#include <type_traits>
 
 #include "internal.h"
 #include "walk.cuh"
@@ -98,6 +99,38 @@ struct Reducer {
 #pragma unroll
       for (int f = 0; f < (NF > 0 ? NF : 1); ++f) out[f] = acc[f];
     }
+  }
+};
+
+// Append one tape entry; the lanes of a warp that reach this point together
+// reserve their slots with one atomic.  Entries past tape_cap are counted
+// but not written (the host then sizes the tape from the count).
+__device__ __forceinline__ void tape_append(const WalkIO& io, int pid, int ray, double ds) {
+  const unsigned m = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(io.tape_count, (unsigned long long)__popc(m));
+  base = __shfl_sync(m, base, leader);
+  const unsigned long long k = base + __popc(m & ((1u << lane) - 1u));
+  if (k < io.tape_cap) io.tape[k] = TapeEntry{pid, ray, ds};
+}
+
+// Reducer of 'integrate' that also records the tape; the first `skip`
+// segments of the ray were recorded by an earlier, handed-over launch.
+template <int MODE, int NF>
+struct TapeReducer : Reducer<MODE, NF> {
+  const WalkIO* io;
+  int ray;
+  unsigned skip;
+  __device__ __forceinline__ void set_tape(const WalkIO* w, int64_t r, unsigned sk) {
+    io = w;
+    ray = (int)r;
+    skip = sk;
+  }
+  __device__ __forceinline__ void seg(int cell, double a, double b) {
+    Reducer<MODE, NF>::seg(cell, a, b);
+    if (this->nseg > skip) tape_append(*io, this->c->perm[cell], ray, dsub(b, a));
   }
 };
 
@@ -220,6 +253,14 @@ __device__ __forceinline__ int run_ray(const DevCloud& c, const WalkIO& io, int6
       red.write(row);
       if (OUT == kOutCount) io.counts[ray] = red.nseg;
     }
+  } else if (OUT == kOutTape) {
+    double* row = io.out + ray * io.nout;
+    TapeReducer<MODE, NF> red;
+    red.init(&c, row);
+    red.set_tape(&io, ray, skip);
+    rc = walk_ray(c, g, io.max_iter, S, st, red, (WalkDiag*)nullptr);
+    nseg = red.nseg;
+    if (rc == 0) red.write(row);
   } else if (OUT == kOutFill) {
     FillSink fs;
     fs.init(&c, io, ray);
@@ -347,9 +388,11 @@ static int launch_walk_t(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) 
     if (kernel == VT_KERNEL_PLAIN_FP64) {
       const int B = 128;
       k_plain<MODE, NF, OUT><<<(unsigned)((io.nrays + B - 1) / B), B, 0, st>>>(c, io);
-    } else if (kernel == VT_KERNEL_BATCHED && cl->nfields <= 32) {
-      int rc = launch_warp<MODE, OUT>(cl, io, st);
-      if (rc) return rc;
+    } else if (OUT != kOutTape && kernel == VT_KERNEL_BATCHED && cl->nfields <= 32) {
+      if constexpr (OUT != kOutTape) {
+        int rc = launch_warp<MODE, OUT>(cl, io, st);
+        if (rc) return rc;
+      }
     } else {
       int rc = launch_batched<MODE, NF, OUT>(cl, io, kernel, st);
       if (rc) return rc;
@@ -416,6 +459,13 @@ static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int ker
     case kOutImage: rc = launch_walk_mode<kOutImage>(cl, io, mode, kernel, st); break;
     case kOutCount: rc = launch_walk_mode<kOutCount>(cl, io, mode, kernel, st); break;
     case kOutFill: rc = launch_walk_t<kSum, 1, kOutFill>(cl, io, kernel, st); break;
+    case kOutTape:
+      if (mode != kSum) return set_error(VT_ERR_INVALID, "a tape is recorded for 'integrate' only");
+      if (cl->nfields == 1) rc = launch_walk_t<kSum, 1, kOutTape>(cl, io, kernel, st);
+      else if (cl->nfields == 3) rc = launch_walk_t<kSum, 3, kOutTape>(cl, io, kernel, st);
+      else if (cl->nfields == 4) rc = launch_walk_t<kSum, 4, kOutTape>(cl, io, kernel, st);
+      else rc = launch_walk_t<kSum, 0, kOutTape>(cl, io, kernel, st);
+      break;
     default: rc = launch_walk_mode<kOutAdj>(cl, io, mode, kernel, st); break;
   }
   if (rc) {
@@ -435,6 +485,7 @@ static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int ker
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   }
+  if (hs.rays > 0) cl->cross_per_ray = (double)hs.crossings / (double)hs.rays;
   if (stats) {
     stats->rays = hs.rays;
     stats->crossings = hs.crossings;
@@ -600,6 +651,58 @@ int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaS
   io.gstack_cap = cl->stack_cap;
   io.slow_threads = slow_threads;
   return run_walk_on(cl, io, out_kind, mode, kernel, st, stats, nullptr, true);
+}
+
+// Adjoint of 'integrate' from a tape: grad[pid, f] += gout[ray, f] * ds for
+// every entry.  The lanes of a warp holding the same cell add their terms
+// first (neighbouring rays cross the same cells), then one atomic per cell.
+template <int NF>
+__global__ void k_tape_scatter(const TapeEntry* __restrict__ t, uint64_t n, int nf_rt,
+                               const double* __restrict__ gout, double* __restrict__ grad) {
+  const int lane = threadIdx.x & 31;
+  const int nf = NF > 0 ? NF : nf_rt;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const uint64_t i = base + threadIdx.x;
+    int pid = -1, ray = 0;
+    double ds = 0.0;
+    if (i < n) {
+      const TapeEntry e = t[i];
+      pid = e.pid;
+      ray = e.ray;
+      ds = e.ds;
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, pid);
+    const bool leader = __ffs(peers) - 1 == lane;
+    for (int f = 0; f < nf; ++f) {
+      const double v = pid >= 0 ? gout[(int64_t)ray * nf + f] * ds : 0.0;
+      double sum = 0.0;
+#pragma unroll 8
+      for (int j = 0; j < 32; ++j) {
+        const double vj = __shfl_sync(0xffffffffu, v, j);
+        if ((peers >> j) & 1u) sum += vj;
+      }
+      if (leader && pid >= 0) atomicAdd(&grad[(int64_t)pid * nf + f], sum);
+    }
+  }
+}
+
+int run_tape_scatter(vt_cloud* cl, const void* tape, uint64_t n, const double* d_gout,
+                     double* d_grad, cudaStream_t st) {
+  if (n == 0) return VT_OK;
+  int dev = 0, nsms = 0;
+  VT_CUDA(cudaGetDevice(&dev));
+  VT_CUDA(cudaDeviceGetAttribute(&nsms, cudaDevAttrMultiProcessorCount, dev));
+  const int B = 256;
+  uint64_t blocks = (n + B - 1) / B;
+  if (blocks > (uint64_t)nsms * 16) blocks = (uint64_t)nsms * 16;
+  const TapeEntry* t = static_cast<const TapeEntry*>(tape);
+  const int nf = (int)cl->nfields;
+  if (nf == 1) k_tape_scatter<1><<<(unsigned)blocks, B, 0, st>>>(t, n, nf, d_gout, d_grad);
+  else if (nf == 3) k_tape_scatter<3><<<(unsigned)blocks, B, 0, st>>>(t, n, nf, d_gout, d_grad);
+  else k_tape_scatter<0><<<(unsigned)blocks, B, 0, st>>>(t, n, nf, d_gout, d_grad);
+  VT_CUDA(cudaGetLastError());
+  return VT_OK;
 }
 
 int run_knn(vt_cloud* cl, const double* d_q, int64_t nq, int k, int64_t* d_ids, double* d_r2,

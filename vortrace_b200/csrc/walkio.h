@@ -11,7 +11,16 @@ struct vt_cloud;
 
 namespace vt {
 
-constexpr int kOutImage = 0, kOutCount = 1, kOutFill = 2, kOutAdj = 3;
+// kOutTape: the image of 'integrate' plus one tape entry per segment
+constexpr int kOutImage = 0, kOutCount = 1, kOutFill = 2, kOutAdj = 3, kOutTape = 4;
+
+// One segment of a taped forward: the adjoint of 'integrate' needs only
+// the cell (original-order internal id), the ray and the segment length.
+struct TapeEntry {
+  int32_t pid;
+  int32_t ray;
+  double ds;
+};
 constexpr int kErrNonFinite = 16;
 
 struct WalkDiag;
@@ -40,6 +49,9 @@ struct WalkIO {
   int local_cap;         // in-register stack entries per ray
   int cache_mode;        // batched kernel: 1 = neighbourhood cache on
   const int32_t* order;  // batched kernels: ray visiting order (NULL: 0..nrays-1)
+  TapeEntry* tape;       // kOutTape: entries [0, tape_cap) of the tape
+  unsigned long long* tape_count;  // kOutTape: entries appended (may exceed tape_cap)
+  unsigned long long tape_cap;
   WalkDiag* diag;
 };
 
