@@ -42,6 +42,7 @@ extern "C" {
 #define VT_ERR_KNN_EXPAND 14   /* src/ray.cpp:331-336 100-NN classification   */
 #define VT_ERR_STACK 15        /* pending-point stack above VT_PARAM_STACK_CAP
                                   (the reference's list is heap-grown)         */
+#define VT_ERR_PERIODIC_BISECT 18 /* src/ray.cpp:243-246 periodic same-cell ray */
 
 /* ---- reduction modes: include/mytypes.hpp:14 (ReductionMode) ----------- */
 #define VT_REDUCE_SUM 0

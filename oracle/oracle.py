@@ -278,10 +278,8 @@ def load_reference_module():
     return None
 
 
-def reference_project(mod, pos, fields, subbox, starts, ends, mode="integrate", vol=None,
-                      detailed=False):
-    """Run the reference's own native path: PointCloud.loadPoints/buildTree,
-    Projection.makeProjection (or makeDetailedProjection + returnSegments)."""
+def reference_cloud(mod, pos, fields, subbox, vol=None, periodic=False):
+    """The reference's PointCloud after loadPoints + buildTree."""
     import warnings as _w
     pc = mod.PointCloud()
     with _w.catch_warnings():
@@ -289,11 +287,20 @@ def reference_project(mod, pos, fields, subbox, starts, ends, mode="integrate", 
         if vol is not None:
             pc.loadPoints(np.ascontiguousarray(pos, np.float64),
                           np.ascontiguousarray(fields, np.float64), list(subbox),
-                          np.ascontiguousarray(vol, np.float64), False)
+                          np.ascontiguousarray(vol, np.float64), bool(periodic))
         else:
             pc.loadPoints(np.ascontiguousarray(pos, np.float64),
-                          np.ascontiguousarray(fields, np.float64), list(subbox))
+                          np.ascontiguousarray(fields, np.float64), list(subbox),
+                          periodic=bool(periodic))
     pc.buildTree()
+    return pc
+
+
+def reference_project(mod, pos, fields, subbox, starts, ends, mode="integrate", vol=None,
+                      detailed=False, periodic=False):
+    """Run the reference's own native path: PointCloud.loadPoints/buildTree,
+    Projection.makeProjection (or makeDetailedProjection + returnSegments)."""
+    pc = reference_cloud(mod, pos, fields, subbox, vol, periodic)
     m = {"integrate": mod.ReductionMode.Sum, "sum": mod.ReductionMode.Sum,
          "max": mod.ReductionMode.Max, "min": mod.ReductionMode.Min,
          "volume": mod.ReductionMode.VolumeRender}[mode]

@@ -14,8 +14,14 @@ has the reference checkout and oracle/_ref built; not needed at test time).
    integrate/max/min/volume outputs produced by the reference module
    (oracle/_ref) on small seeded clouds: uniform, Plummer-clustered, a cubic
    lattice with degenerate rays, and float32-quantised positions.
+3. ``periodic_walks.npz``: the same for periodic clouds (loadPoints with
+   periodic=True): a uniform cloud with rays across the domain faces, rays
+   leaving the domain and rays whose two ends lie in one cell (the
+   same-cell bisection), the reference's periodic k-NN (queryTree(q, k))
+   for queries inside, near and outside the domain, and a cubic lattice
+   (tests/test_periodic.py in the reference).
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py [/path/to/reference [galaxy|small|periodic ...]]
 """
 from __future__ import annotations
 
@@ -173,14 +179,93 @@ def small_walks(mod):
     print("small_walks.npz written")
 
 
+def periodic_walks(mod):
+    rng = np.random.default_rng(20240707)
+    blob = {}
+    # uniform cloud in [0, 10)^3
+    n = 2000
+    pos = rng.uniform(0, 10, (n, 3))
+    rho = rng.lognormal(0, 1, n)
+    st = [rng.uniform(0, 10, (60, 3))]
+    en = [rng.uniform(0, 10, (60, 3))]
+    for ax in range(3):  # rays hugging the faces normal to each axis
+        a = rng.uniform(0, 10, (8, 3))
+        b = rng.uniform(0, 10, (8, 3))
+        a[:, ax] = rng.uniform(0.005, 0.05, 8)
+        b[:, ax] = rng.uniform(9.95, 9.995, 8)
+        st.append(a)
+        en.append(b)
+    # rays whose ends sit next to one generator and next to its periodic
+    # image: both ends in one cell, so the walk bisects for another cell
+    for ax in range(3):
+        order = np.argsort(pos[:, ax])[:4]
+        for i in order:
+            a = pos[i].copy()
+            b = pos[i].copy()
+            a[ax] += 0.01
+            b[ax] += 10.0 - 0.01
+            st.append(a[None])
+            en.append(b[None])
+    # rays leaving the domain
+    a = rng.uniform(0, 10, (8, 3))
+    b = rng.uniform(0, 10, (8, 3))
+    a[:, 0] = -1.5
+    b[:, 0] = 11.5
+    st.append(a)
+    en.append(b)
+    st = np.vstack(st)
+    en = np.vstack(en)
+    out, segs, oid = O.reference_project(mod, pos, rho, [0, 10] * 3, st, en, detailed=True,
+                                         periodic=True)
+    cid, se, sx, off = segs
+    blob.update({"uniform/pos": pos, "uniform/fields": rho, "uniform/bb": np.array([0, 10.0] * 3),
+                 "uniform/starts": st, "uniform/ends": en,
+                 "uniform/out": np.asarray(out).reshape(len(st), -1),
+                 "uniform/cell_ids": np.asarray(cid, np.int64), "uniform/s_enter": np.asarray(se),
+                 "uniform/s_exit": np.asarray(sx), "uniform/offsets": np.asarray(off, np.int64),
+                 "uniform/orig_ids": np.asarray(oid, np.int64)})
+    print("periodic uniform segments:", len(cid))
+    pc = O.reference_cloud(mod, pos, rho, [0, 10] * 3, periodic=True)
+    q = np.vstack([rng.uniform(-0.5, 10.5, (240, 3)),
+                   np.array([[x, y, z] for x in (0.01, 9.99) for y in (0.02, 9.98)
+                             for z in (0.03, 9.97)])])
+    blob["uniform/knn_q"] = q
+    for k in (1, 3, 10):
+        ids = np.zeros((len(q), k), np.int64)
+        r2 = np.zeros((len(q), k))
+        for i, qq in enumerate(q):
+            a, b = pc.queryTree(qq, k)
+            ids[i], r2[i] = a, b
+        blob[f"uniform/knn{k}_ids"] = ids
+        blob[f"uniform/knn{k}_r2"] = r2
+    # cubic lattice, box 5, spacing 0.5 (tests/test_periodic.py:10-18)
+    c = np.arange(0.25, 5.0, 0.5)
+    xx, yy, zz = np.meshgrid(c, c, c, indexing="ij")
+    lpos = np.column_stack([xx.ravel(), yy.ravel(), zz.ravel()])
+    lst = np.array([[0.01, 2.5, 2.5], [0.5, 2.5, 2.5], [0.3, 0.4, 0.2], [4.9, 0.1, 2.6]])
+    len_ = np.array([[4.99, 2.5, 2.5], [4.5, 2.5, 2.5], [4.6, 4.7, 4.9], [0.2, 4.8, 2.4]])
+    lout, lsegs, loid = O.reference_project(mod, lpos, np.full(len(lpos), 2.5), [0, 5.0] * 3,
+                                            lst, len_, detailed=True, periodic=True)
+    blob.update({"lattice/pos": lpos, "lattice/bb": np.array([0, 5.0] * 3), "lattice/starts": lst,
+                 "lattice/ends": len_, "lattice/out": np.asarray(lout).reshape(len(lst), -1),
+                 "lattice/offsets": np.asarray(lsegs[3], np.int64)})
+    np.savez_compressed(os.path.join(HERE, "periodic_walks.npz"), **blob)
+    print("periodic_walks.npz written")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     mod = O.load_reference_module()
     if mod is None:
         raise SystemExit("oracle/_ref/Cvortrace not built: run oracle/build_ref.sh first")
     warnings.simplefilter("ignore")
-    galaxy(ref_root, mod)
-    small_walks(mod)
+    which = sys.argv[2:] or ["galaxy", "small", "periodic"]
+    if "galaxy" in which:
+        galaxy(ref_root, mod)
+    if "small" in which:
+        small_walks(mod)
+    if "periodic" in which:
+        periodic_walks(mod)
 
 
 if __name__ == "__main__":

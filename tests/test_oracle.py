@@ -157,3 +157,20 @@ def test_load_points_matches_reference(ref_module):
         lp = O.load_points(pos, np.ones(3000), [10, 90, 0, 100, 20, 60], v)
         np.testing.assert_array_equal(np.asarray(pc.get_orig_ids()), lp["orig_ids"])
         assert pc.get_pad() == lp["pad"]
+
+
+def test_periodic_fixture_consistency():
+    """The reference-generated periodic fixture: CSR offsets, segments that
+    tile every ray, and the lattice's density x length."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "periodic_walks.npz"))
+    st, en, off = z["uniform/starts"], z["uniform/ends"], z["uniform/offsets"]
+    L = np.linalg.norm(en - st, axis=1)
+    assert off[0] == 0 and np.all(np.diff(off) >= 1) and off[-1] == len(z["uniform/cell_ids"])
+    ds = z["uniform/s_exit"] - z["uniform/s_enter"]
+    for i in range(len(st)):
+        np.testing.assert_allclose(np.sum(ds[off[i]:off[i + 1]]), L[i], rtol=1e-12)
+    # same-cell rays (both ends next to one generator) cross other cells
+    assert np.all(np.diff(off)[84:96] > 1)
+    Ll = np.linalg.norm(z["lattice/ends"] - z["lattice/starts"], axis=1)
+    np.testing.assert_allclose(z["lattice/out"][:, 0], 2.5 * Ll, rtol=1e-10)

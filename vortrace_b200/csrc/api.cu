@@ -75,9 +75,6 @@ int vt::check_projectable(const vt_cloud* cl, int mode) {
       return set_error(VT_ERR_INVALID,
                        "Volume rendering requires R, G, B values in [0, 1] and alpha >= 0");
   }
-  if (cl->periodic)
-    return set_error(VT_ERR_RUNTIME,
-                     "periodic projections are not supported by libvortrace_b200 yet");
   return VT_OK;
 }
 

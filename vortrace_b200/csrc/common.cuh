@@ -38,6 +38,7 @@ constexpr int kErrPerturb = 13;
 constexpr int kErrKnnExpand = 14;
 constexpr int kErrStack = 15;
 constexpr int kErrNonFiniteDist = 17;  // squared distances overflowed
+constexpr int kErrPeriodicBisect = 18;  // no second cell on a periodic same-cell ray
 // internal: the ray must be finished by the degenerate-geometry kernel
 constexpr int kNeedSlow = 99;
 
@@ -62,6 +63,9 @@ struct DevCloud {
   double origin[3];         // frame of pts32 / nodes32
   float bblo32[3], bbhi32[3];  // root box in that frame, rounded outward
   float coord_err;          // bound on |pts32 - (p - origin)| per component
+  // periodic domain (src/pointcloud.cpp:26-32): the subbox and its side lengths
+  int periodic;
+  double sub_lo[3], sub_hi[3], box[3];
 };
 
 // ---- FP64 arithmetic with the reference's rounding (no FMA contraction) --

@@ -57,6 +57,9 @@ struct KnnList {
     for (int j = 0; j < K; ++j) c += (id[j] >= 0);
     return c;
   }
+  __device__ __forceinline__ int capacity() const { return K; }
+  __device__ __forceinline__ void clear(int) { clear(); }
+  __device__ __forceinline__ void set_count(int) {}
 };
 
 // Runtime-k list for the rare large queries (k up to KMAX, local memory).
@@ -90,6 +93,8 @@ struct KnnBig {
     if (cnt < k) ++cnt;
   }
   __device__ __forceinline__ int count() const { return cnt; }
+  __device__ __forceinline__ int capacity() const { return k; }
+  __device__ __forceinline__ void set_count(int n) { cnt = n; }
 };
 
 // Depth-first, nearer-child-first exact search (nanoflann's traversal on the
@@ -179,12 +184,115 @@ __device__ __noinline__ void knn_exact64(const DevCloud& c, double qx, double qy
   nvisit += visits;
 }
 
-// Convenience: nearest neighbour (tree index) of q.
+// PointCloud::minDistSqToBox (src/pointcloud.cpp:283-297)
+__device__ __forceinline__ double min_dist_sq_to_box(const DevCloud& c, double x, double y,
+                                                     double z) {
+  const double q[3] = {x, y, z};
+  double d2 = 0.0;
+#pragma unroll
+  for (int dim = 0; dim < 3; dim++) {
+    const double lo = c.sub_lo[dim], hi = c.sub_hi[dim];
+    if (q[dim] < lo) {
+      const double d = dsub(lo, q[dim]);
+      d2 = dadd(d2, dmul(d, d));
+    } else if (q[dim] > hi) {
+      const double d = dsub(q[dim], hi);
+      d2 = dadd(d2, dmul(d, d));
+    }
+  }
+  return d2;
+}
+
+// Periodic images of PointCloud::queryTreeK (src/pointcloud.cpp:308-368):
+// `res` holds the k-NN of q itself; each of the 26 shifted queries whose
+// distance to the domain is within the current k-th distance + TOL is
+// searched too, and the results are merged: one entry per particle with
+// its smallest distance, sorted ascending, truncated to k.  (Equal
+// distances keep their merge order here; the reference's std::sort leaves
+// their order unspecified.)  `L` is KnnList<K> or KnnBig<KMAX>.
+template <int KMAX, class L>
+__device__ __noinline__ void knn_periodic_merge64(const DevCloud& c, double qx, double qy,
+                                                  double qz, L& res, unsigned& nvisit) {
+  const int k = res.capacity();
+  double md[2 * KMAX];
+  int mi[2 * KMAX];
+  int mn = res.count();
+  for (int i = 0; i < mn; i++) {
+    md[i] = res.r2[i];
+    mi[i] = res.id[i];
+  }
+  for (int ix = -1; ix <= 1; ix++) {
+    for (int iy = -1; iy <= 1; iy++) {
+      for (int iz = -1; iz <= 1; iz++) {
+        if (ix == 0 && iy == 0 && iz == 0) continue;
+        const double sx = dadd(qx, dmul((double)ix, c.box[0]));
+        const double sy = dadd(qy, dmul((double)iy, c.box[1]));
+        const double sz = dadd(qz, dmul((double)iz, c.box[2]));
+        const double minD2 = min_dist_sq_to_box(c, sx, sy, sz);
+        const double worst = mn >= k ? md[k - 1] : __longlong_as_double(0x7ff0000000000000ULL);
+        if (minD2 > dadd(worst, kTol)) continue;
+        L img;
+        img.clear(k);
+        knn_exact64(c, sx, sy, sz, __longlong_as_double(0x7ff0000000000000ULL), img, nvisit);
+        const int ni = img.count();
+        for (int i = 0; i < ni; i++) {
+          bool found = false;
+          for (int m = 0; m < mn; m++) {
+            if (mi[m] == img.id[i]) {
+              md[m] = fmin(md[m], img.r2[i]);
+              found = true;
+              break;
+            }
+          }
+          if (!found) {
+            md[mn] = img.r2[i];
+            mi[mn] = img.id[i];
+            ++mn;
+          }
+        }
+        // sort ascending (stable insertion sort) and truncate to k
+        for (int a = 1; a < mn; a++) {
+          const double d = md[a];
+          const int id = mi[a];
+          int b = a;
+          for (; b > 0 && md[b - 1] > d; --b) {
+            md[b] = md[b - 1];
+            mi[b] = mi[b - 1];
+          }
+          md[b] = d;
+          mi[b] = id;
+        }
+        if (mn > k) mn = k;
+      }
+    }
+  }
+  for (int i = 0; i < mn; i++) {
+    res.r2[i] = md[i];
+    res.id[i] = mi[i];
+  }
+  res.set_count(mn);
+}
+
+// The k-NN of the reference's queryTreeK: exact FP64 search, then, in code
+// compiled with PER and on a periodic cloud, the periodic merge.  Kernels
+// that never serve periodic clouds compile without it (PER = false), which
+// keeps the merge out of their register allocation.
+template <int KMAX, bool PER, class L>
+__device__ __forceinline__ void knn_query64(const DevCloud& c, double qx, double qy, double qz,
+                                            L& res, unsigned& nvisit) {
+  knn_exact64(c, qx, qy, qz, __longlong_as_double(0x7ff0000000000000ULL), res, nvisit);
+  if constexpr (PER) {
+    if (c.periodic && res.count() > 0) knn_periodic_merge64<KMAX>(c, qx, qy, qz, res, nvisit);
+  }
+}
+
+// Nearest neighbour (tree index) of q.
+template <bool PER = false>
 __device__ __forceinline__ int nn1_exact64(const DevCloud& c, double qx, double qy, double qz,
                                            unsigned& nvisit) {
   KnnList<1> r;
   r.clear();
-  knn_exact64(c, qx, qy, qz, __longlong_as_double(0x7ff0000000000000ULL), r, nvisit);
+  knn_query64<1, PER>(c, qx, qy, qz, r, nvisit);
   return r.id[0];
 }
 

@@ -286,11 +286,11 @@ __device__ __forceinline__ void hand_over(const WalkIO& io, int64_t ray, unsigne
 }
 
 // ------------------------------------------------------------ k_plain
-template <int MODE, int NF, int OUT>
+template <int MODE, int NF, int OUT, bool PER>
 __global__ void __launch_bounds__(128) k_plain(DevCloud c, WalkIO io) {
   const int64_t ray = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (ray >= io.nrays) return;
-  Search64 S(c);
+  Search64T<PER> S(c);
   LocalStack<kPlainStack> st;
   st.set_cap(io.local_cap);
   st.clear();
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(128) k_plain(DevCloud c, WalkIO io) {
 }
 
 // ------------------------------------------------------------- k_slow
-template <int MODE, int NF, int OUT>
+template <int MODE, int NF, int OUT, bool PER>
 __global__ void __launch_bounds__(128) k_slow(DevCloud c, WalkIO io) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   GlobalStack st;
@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(128) k_slow(DevCloud c, WalkIO io) {
     const unsigned long long e = io.slow_q[q];
     const int64_t ray = (int64_t)(e >> 24);
     const unsigned skip = (unsigned)(e & 0xffffffu);
-    Search64 S(c);
+    Search64T<PER> S(c);
     unsigned nseg = 0;
     int rc = run_ray<MODE, NF, OUT>(c, io, ray, S, st, skip, nseg);
     if (rc == kNeedSlow) rc = kErrStack;
@@ -344,7 +344,7 @@ __global__ void k_diag(DevCloud c, WalkIO io, int64_t ray) {
     io.diag->code = kErrNonFinite;
     return;
   }
-  Search64 S(c);
+  Search64T<true> S(c);  // serves periodic and non-periodic clouds
   NullSink ns;
   int rc = walk_ray(c, g, io.max_iter, S, st, ns, io.diag);
   if (rc == kNeedSlow) rc = kErrStack;
@@ -363,7 +363,7 @@ __global__ void k_knn(DevCloud c, const double* __restrict__ q, int64_t nq, int 
   KnnBig<128> r;
   r.clear(k);
   unsigned v = 0;
-  knn_exact64(c, q[3 * i], q[3 * i + 1], q[3 * i + 2], pinf(), r, v);
+  knn_query64<128, true>(c, q[3 * i], q[3 * i + 1], q[3 * i + 2], r, v);
   for (int j = 0; j < k; ++j) {
     const bool ok = j < r.cnt;
     ids[i * k + j] = ok ? (int64_t)c.perm[r.id[j]] : -1;
@@ -385,9 +385,11 @@ template <int MODE, int NF, int OUT>
 static int launch_walk_t(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) {
   const DevCloud& c = cl->view;
   if (io.nrays > 0) {
-    if (kernel == VT_KERNEL_PLAIN_FP64) {
-      const int B = 128;
-      k_plain<MODE, NF, OUT><<<(unsigned)((io.nrays + B - 1) / B), B, 0, st>>>(c, io);
+    const int B = 128;
+    if (cl->periodic) {
+      k_plain<MODE, NF, OUT, true><<<(unsigned)((io.nrays + B - 1) / B), B, 0, st>>>(c, io);
+    } else if (kernel == VT_KERNEL_PLAIN_FP64) {
+      k_plain<MODE, NF, OUT, false><<<(unsigned)((io.nrays + B - 1) / B), B, 0, st>>>(c, io);
     } else if (OUT != kOutTape && kernel == VT_KERNEL_BATCHED && cl->nfields <= 32) {
       if constexpr (OUT != kOutTape) {
         int rc = launch_warp<MODE, OUT>(cl, io, st);
@@ -399,7 +401,10 @@ static int launch_walk_t(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) 
     }
     VT_CUDA(cudaGetLastError());
     const int SB = 128;
-    k_slow<MODE, NF, OUT><<<(unsigned)(io.slow_threads / SB), SB, 0, st>>>(c, io);
+    if (cl->periodic)
+      k_slow<MODE, NF, OUT, true><<<(unsigned)(io.slow_threads / SB), SB, 0, st>>>(c, io);
+    else
+      k_slow<MODE, NF, OUT, false><<<(unsigned)(io.slow_threads / SB), SB, 0, st>>>(c, io);
     VT_CUDA(cudaGetLastError());
   }
   return VT_OK;
@@ -442,6 +447,12 @@ static std::string fmt_double(double v) {
 // the launches for vt_stats.walk_ms.
 static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel,
                        cudaStream_t st, vt_stats* stats, WalkDiag* d_diag, bool timed) {
+  // periodic clouds: the periodic k-NN merge and minimum-image split points
+  // live in the exact FP64 walk of the one-ray-per-thread kernel
+  if (cl->periodic) {
+    kernel = VT_KERNEL_PLAIN_FP64;
+    io.order = nullptr;
+  }
   io.max_iter = cl->max_iter;
   io.local_cap = cl->local_stack;
   io.cache_mode = cl->cache_mode;
@@ -547,6 +558,9 @@ static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int ker
       case kErrNonFiniteDist:
         return set_error(VT_ERR_INVALID, "Squared distances overflow for ray " +
                                              std::to_string(ray) + ": coordinates too large");
+      case kErrPeriodicBisect:
+        msg = "Could not find intermediate cell by bisection along periodic ray";
+        break;
       default: msg = "ray walk failed with code " + std::to_string(code); break;
     }
     return set_error(code, msg);
@@ -554,7 +568,6 @@ static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int ker
   return VT_OK;
 }
 
-// Walk launch with the handle's (grow-only) workspace as scratch.
 // ------------------------------------------------------- ray ordering
 // The batched kernels walk the rays in a coherent order: sorted by a 64-bit
 // key of the quantized direction (5 bits per component, bits 48-62) and the
@@ -631,9 +644,10 @@ static int sort_rays(vt_cloud* cl, WalkIO& io, cudaStream_t st) {
   return VT_OK;
 }
 
+// Walk launch with the handle's (grow-only) workspace as scratch.
 int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaStream_t st,
              vt_stats* stats) {
-  if (kernel != VT_KERNEL_PLAIN_FP64) {
+  if (kernel != VT_KERNEL_PLAIN_FP64 && !cl->periodic) {
     const int rc = sort_rays(cl, io, st);
     if (rc) return rc;
   } else {

@@ -481,6 +481,12 @@ int build_tree_device(vt_cloud* cl) {
   }
   // |fl32(p - o) - (p - o)| <= 2^-24 |p - o| (plus the FP64 subtraction)
   v.coord_err = (float)(mext * 6.0e-8 + 1e-300);
+  v.periodic = cl->periodic ? 1 : 0;
+  for (int j = 0; j < 3; ++j) {
+    v.sub_lo[j] = cl->subbox[2 * j];
+    v.sub_hi[j] = cl->subbox[2 * j + 1];
+    v.box[j] = cl->subbox[2 * j + 1] - cl->subbox[2 * j];
+  }
   return VT_OK;
 #undef VT_TRY
 }

@@ -112,38 +112,62 @@ struct GlobalStack {
 };
 
 // ------------------------------------------------------- exact FP64 search
-// Full-featured search policy (plain kernel and degenerate-geometry kernel).
-struct Search64 {
+// Full-featured search policy (plain kernel and degenerate-geometry kernel);
+// PER: also serves periodic clouds (periodic k-NN merge, minimum-image split
+// points, same-cell bisection).
+template <bool PER>
+struct Search64T {
   const DevCloud& c;
   unsigned nq = 0, nvisit = 0;
-  __device__ explicit Search64(const DevCloud& cc) : c(cc) {}
+  static constexpr bool kPeriodic = PER;
+  __device__ explicit Search64T(const DevCloud& cc) : c(cc) {}
   __device__ __forceinline__ int nn1(double x, double y, double z) {
     ++nq;
-    return nn1_exact64(c, x, y, z, nvisit);
+    return nn1_exact64<PER>(c, x, y, z, nvisit);
   }
   // 3-NN at a split point between cells cid and nid
   __device__ __forceinline__ int knn3(double x, double y, double z, int cid, int nid,
                                       KnnList<3>& r) {
     ++nq;
     r.clear();
-    knn_exact64(c, x, y, z, __longlong_as_double(0x7ff0000000000000ULL), r, nvisit);
+    knn_query64<3, PER>(c, x, y, z, r, nvisit);
     return 0;
   }
   __device__ __forceinline__ void knn2(double x, double y, double z, KnnList<2>& r) {
     ++nq;
     r.clear();
-    knn_exact64(c, x, y, z, __longlong_as_double(0x7ff0000000000000ULL), r, nvisit);
+    knn_query64<2, PER>(c, x, y, z, r, nvisit);
   }
   static constexpr bool kDefer = false;  // rare paths run inline
 };
+using Search64 = Search64T<false>;
 
 // ------------------------------------------------------------------ walk
 // Ray::findSplitPointDistance(cloud, id1, id2, s_lo, s_hi) (src/ray.cpp:64-127)
 template <class S>
 __device__ int split_full(const DevCloud& c, const RayGeom& g, S& srch, int id1, int id2,
                           double s_lo, double s_hi, double& s_out) {
-  const double4 p1 = ldg_pt(&c.pts[id1]);
-  const double4 p2 = ldg_pt(&c.pts[id2]);
+  double4 p1 = ldg_pt(&c.pts[id1]);
+  double4 p2 = ldg_pt(&c.pts[id2]);
+  if (S::kPeriodic && c.periodic) {
+    // minimum image of both generators about the segment's midpoint on the
+    // ray (src/ray.cpp:71-86)
+    const double s_ref = dmul(0.5, dadd(s_lo, s_hi));
+    double a[3] = {p1.x, p1.y, p1.z}, b[3] = {p2.x, p2.y, p2.z};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const double ref = dadd(g.s[d], dmul(s_ref, g.d[d]));
+      const double half = dmul(c.box[d], 0.5);
+      const double diff1 = dsub(a[d], ref);
+      if (diff1 > half) a[d] = dsub(a[d], c.box[d]);
+      else if (diff1 < -half) a[d] = dadd(a[d], c.box[d]);
+      const double diff2 = dsub(b[d], ref);
+      if (diff2 > half) b[d] = dsub(b[d], c.box[d]);
+      else if (diff2 < -half) b[d] = dadd(b[d], c.box[d]);
+    }
+    p1 = make_double4(a[0], a[1], a[2], 0.0);
+    p2 = make_double4(b[0], b[1], b[2], 0.0);
+  }
   double s = split_analytic(g, p1, p2);
   if (s < DBL_MAX * 0.5 && s >= s_lo - kTol && s <= s_hi + kTol) {
     s_out = s;
@@ -230,13 +254,14 @@ __device__ int try_along_ray(const RayGeom& g, S& srch, double px, double py, do
 }
 
 // 100-NN expansion (src/ray.cpp:319-338).  Returns 0 or kErrKnnExpand.
+template <bool PER = false>
 __device__ __noinline__ int expand_classify(const DevCloud& c, double x, double y, double z,
                                             int cid, int nid, bool& has_c, bool& has_n,
                                             unsigned& nvisit) {
   KnnBig<kExpandK> r;
   const int kb = (int)min((int64_t)kExpandK, c.n);
   r.clear(kb);
-  knn_exact64(c, x, y, z, __longlong_as_double(0x7ff0000000000000ULL), r, nvisit);
+  knn_query64<kExpandK, PER>(c, x, y, z, r, nvisit);
   for (int i = 0; i < kb; i++) {
     if (dsub(r.r2[i], r.r2[0]) >= kTol) break;
     if (r.id[i] == cid) has_c = true;
@@ -246,7 +271,7 @@ __device__ __noinline__ int expand_classify(const DevCloud& c, double x, double 
   return 0;
 }
 
-// Ray::walk (src/ray.cpp:187-430), non-periodic.  Emits segments in order to
+// Ray::walk (src/ray.cpp:187-430).  Emits segments in order to
 // `sink.seg(cell, s_enter, s_exit)`.  Returns 0, an error code, or kNeedSlow
 // (search policy with kDefer, or a stack without room).
 template <class S, class Stack, class Sink>
@@ -257,12 +282,36 @@ __device__ int walk_ray(const DevCloud& c, const RayGeom& g, int64_t max_iter, S
   if (c0 < 0 || c1 < 0) return kErrNonFiniteDist;  // squared distances overflowed
   int open_cell = c0;
   double entry_s = 0.0;
-  if (c0 == c1) {
-    sink.seg(c0, 0.0, g.len);
-    return 0;
-  }
   st.clear();
   st.push(c1, g.len);
+  if (c0 == c1) {
+    if (!(S::kPeriodic && c.periodic)) {
+      sink.seg(c0, 0.0, g.len);
+      return 0;
+    }
+    // periodic: sample the ray at dyadic fractions 1/2, 1/4, 3/4, 1/8, ...
+    // for a point in another cell and walk towards it first
+    // (src/ray.cpp:220-246)
+    bool found = false;
+    for (int level = 1; level <= 10 && !found; level++) {
+      const int n = 1 << level;
+      for (int i = 1; i < n && !found; i += 2) {
+        const double mid_s = ddiv(dmul(g.len, (double)i), (double)n);
+        double x, y, z;
+        ray_point(g, mid_s, x, y, z);
+        const int mc = srch.nn1(x, y, z);
+        if (mc < 0) return kErrNonFiniteDist;
+        if (mc != c0) {
+          st.push(mc, mid_s);
+          found = true;
+        }
+      }
+    }
+    if (!found) {
+      if (diag) diag->code = kErrPeriodicBisect;
+      return kErrPeriodicBisect;
+    }
+  }
   int cur = c0;
   double cur_s = 0.0;
   int64_t iteration = 0;
@@ -325,7 +374,7 @@ __device__ int walk_ray(const DevCloud& c, const RayGeom& g, int64_t max_iter, S
     }
     if (three_eq && !has_c && !has_n) {
       if (S::kDefer) return kNeedSlow;
-      rc = expand_classify(c, x, y, z, cur, nxt, has_c, has_n, srch.nvisit);
+      rc = expand_classify<S::kPeriodic>(c, x, y, z, cur, nxt, has_c, has_n, srch.nvisit);
       if (rc) {
         if (diag) diag->code = rc;
         return rc;
