@@ -211,6 +211,19 @@ int vt_project_adjoint_device(vt_cloud *cloud, const double *d_starts, const dou
                               uint64_t nrays, int mode, const double *d_out,
                               const double *d_grad_out, double *d_grad_fields, void *stream);
 
+/* Slice::makeSlice (src/slice.cpp:6-60, src/bindings.cpp:259-273): out[(i *
+ * npix[1] + j) * nfields + f] = field f of the cell nearest to (extent[0] +
+ * i dx, extent[2] + j dy, depth), dx = (extent[1] - extent[0]) / (npix[0] -
+ * 1); extent = {xmin, xmax, ymin, ymax} must lie in the cloud's subbox. */
+int vt_slice(vt_cloud *cloud, const uint64_t npix[2], const double extent[4], double depth,
+             double *out);
+/* BruteProjection::makeProjection (src/brute_projection.cpp:10-96,
+ * src/bindings.cpp:240-257): per pixel (i, j), SUM (times dz), MAX or MIN
+ * of the nearest cells' fields at the npix[2] depth samples; extent = {xmin,
+ * xmax, ymin, ymax, zmin, zmax}.  out: npix[0] * npix[1] * nfields. */
+int vt_brute_projection(vt_cloud *cloud, const uint64_t npix[3], const double extent[6],
+                        int mode, double *out);
+
 /* Segment tape (no reference counterpart; the reference has no gradients).
  * vt_project_device_tape is vt_project_device for SUM that also records, in
  * device memory owned by the tape, one (cell, ray, ds) entry per segment --

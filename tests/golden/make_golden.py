@@ -20,8 +20,11 @@ has the reference checkout and oracle/_ref built; not needed at test time).
    same-cell bisection), the reference's periodic k-NN (queryTree(q, k))
    for queries inside, near and outside the domain, and a cubic lattice
    (tests/test_periodic.py in the reference).
+4. ``slice_brute.npz``: Slice.makeSlice and BruteProjection.makeProjection
+   (sum, max, min) of the reference module on a seeded uniform cloud with two
+   fields, and a slice of its periodic counterpart.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference [galaxy|small|periodic ...]]
+Usage:  python tests/golden/make_golden.py [/path/to/reference [galaxy|small|periodic|slice ...]]
 """
 from __future__ import annotations
 
@@ -253,19 +256,50 @@ def periodic_walks(mod):
     print("periodic_walks.npz written")
 
 
+def slice_brute(mod):
+    rng = np.random.default_rng(20240808)
+    n = 3000
+    pos = rng.uniform(0, 10, (n, 3))
+    f = np.column_stack([rng.lognormal(0, 1, n), rng.uniform(0, 1, n)])
+    blob = {"pos": pos, "fields": f, "bb": np.array([0, 10.0] * 3)}
+    slices = [((37, 23), [0.5, 9.5, 1.0, 9.0], 3.3), ((16, 16), [0.0, 10.0, 0.0, 10.0], 0.0),
+              ((9, 31), [2.0, 8.0, 2.0, 8.0], 10.0)]
+    for periodic in (False, True):
+        pc = O.reference_cloud(mod, pos, f, [0, 10] * 3, periodic=periodic)
+        tag = "periodic" if periodic else "open"
+        for i, (npix, ext, depth) in enumerate(slices):
+            sl = mod.Slice(list(npix), list(ext), depth)
+            sl.makeSlice(pc)
+            blob[f"{tag}/slice{i}"] = np.asarray(sl.returnSlice()).reshape(npix[0] * npix[1], -1)
+        if not periodic:
+            for mode in ("Sum", "Max", "Min"):
+                bp = mod.BruteProjection([12, 10, 25], [1.0, 9.0, 1.0, 9.0, 0.0, 10.0])
+                bp.makeProjection(pc, getattr(mod.ReductionMode, mode))
+                blob[f"open/brute_{mode.lower()}"] = np.asarray(bp.returnProjection()).reshape(
+                    120, -1)
+    for i, (npix, ext, depth) in enumerate(slices):
+        blob[f"slice{i}/npix"] = np.array(npix)
+        blob[f"slice{i}/extent"] = np.array(ext)
+        blob[f"slice{i}/depth"] = np.array(depth)
+    np.savez_compressed(os.path.join(HERE, "slice_brute.npz"), **blob)
+    print("slice_brute.npz written")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     mod = O.load_reference_module()
     if mod is None:
         raise SystemExit("oracle/_ref/Cvortrace not built: run oracle/build_ref.sh first")
     warnings.simplefilter("ignore")
-    which = sys.argv[2:] or ["galaxy", "small", "periodic"]
+    which = sys.argv[2:] or ["galaxy", "small", "periodic", "slice"]
     if "galaxy" in which:
         galaxy(ref_root, mod)
     if "small" in which:
         small_walks(mod)
     if "periodic" in which:
         periodic_walks(mod)
+    if "slice" in which:
+        slice_brute(mod)
 
 
 if __name__ == "__main__":

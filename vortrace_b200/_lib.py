@@ -44,7 +44,7 @@ EXPORTS = (
     "vt_segments_count",
     "vt_segments_copy", "vt_segments_free", "vt_project_adjoint", "vt_project_adjoint_device",
     "vt_tape_create", "vt_tape_destroy", "vt_tape_size", "vt_project_device_tape",
-    "vt_tape_adjoint_device",
+    "vt_tape_adjoint_device", "vt_slice", "vt_brute_projection",
 )
 
 
@@ -129,6 +129,8 @@ def load(path: str | None = None):
         L.vt_tape_create.argtypes = [vp, C.POINTER(vp)]
         L.vt_tape_destroy.argtypes = [vp]
         L.vt_tape_destroy.restype = None
+        L.vt_slice.argtypes = [vp, C.POINTER(u64), dp, C.c_double, dp]
+        L.vt_brute_projection.argtypes = [vp, C.POINTER(u64), dp, C.c_int, dp]
         L.vt_tape_size.argtypes = [vp]
         L.vt_tape_size.restype = u64
         L.vt_project_device_tape.argtypes = [vp, vp, vp, vp, u64, C.c_int, C.c_int, vp, vp,
@@ -140,7 +142,8 @@ def load(path: str | None = None):
                      "vt_project_device", "vt_project_device_noalloc", "vt_project_detailed",
                      "vt_segments_copy",
                      "vt_project_adjoint", "vt_project_adjoint_device", "vt_set_device",
-                     "vt_tape_create", "vt_project_device_tape", "vt_tape_adjoint_device"):
+                     "vt_tape_create", "vt_project_device_tape", "vt_tape_adjoint_device",
+                     "vt_slice", "vt_brute_projection"):
             getattr(L, name).restype = C.c_int
         L.vt_set_warning_callback(_warn_cb)
         _lib = L

@@ -24,6 +24,9 @@ int scan_offsets(vt_cloud* cl, const int64_t* d_counts, int64_t* d_offsets, int6
                  cudaStream_t st);
 int run_tape_scatter(vt_cloud* cl, const void* tape, uint64_t n, const double* d_gout,
                      double* d_grad, cudaStream_t st);
+int run_grid_sample(vt_cloud* cl, bool brute, int mode, const uint64_t* npix, const double* lo,
+                    const double* step, double depth, double* d_out, unsigned long long* d_bad,
+                    cudaStream_t st);
 }  // namespace vt
 
 namespace {
@@ -577,6 +580,78 @@ int vt_project_adjoint_device(vt_cloud* cl, const double* d_starts, const double
   if (nrays == 0) return VT_OK;
   return adjoint_locked(cl, d_starts, d_ends, nrays, mode, d_out, d_grad_out, d_grad_fields,
                         pick_stream(cl, stream));
+  VT_GUARD_END
+}
+
+// Slice / BruteProjection: grid of nearest-cell samples, host buffers.
+static int grid_sample(vt_cloud* cl, bool brute, int mode, const uint64_t* npix,
+                       const double* lo, const double* step, double depth, double* out) {
+  const uint64_t n = npix[0] * npix[1];
+  const uint64_t nf = cl->nfields;
+  int rc;
+  if ((rc = cl->ws_out.reserve(n * nf))) return rc;
+  if ((rc = cl->ws_slow.reserve(1))) return rc;
+  cudaStream_t st = cl->stream;
+  VT_CUDA(cudaMemsetAsync(cl->ws_slow.p, 0xff, sizeof(unsigned long long), st));
+  if ((rc = vt::run_grid_sample(cl, brute, mode, npix, lo, step, depth, cl->ws_out.p,
+                                cl->ws_slow.p, st)))
+    return rc;
+  unsigned long long bad = 0;
+  VT_CUDA(cudaMemcpyAsync(&bad, cl->ws_slow.p, sizeof(bad), cudaMemcpyDeviceToHost, st));
+  if (n * nf > 0)
+    VT_CUDA(cudaMemcpyAsync(out, cl->ws_out.p, n * nf * sizeof(double), cudaMemcpyDeviceToHost,
+                            st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  if (bad != ~0ULL)
+    return set_error(VT_ERR_INVALID, "pixel " + std::to_string(bad) +
+                                         " has no finite distance to any cell (non-finite "
+                                         "sample position)");
+  return VT_OK;
+}
+
+int vt_slice(vt_cloud* cl, const uint64_t npix[2], const double extent[4], double depth,
+             double* out) {
+  VT_GUARD_BEGIN
+  if (!cl || !npix || !extent || !out) return set_error(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  // src/slice.cpp:9-21
+  if (!cl->tree_built)
+    return set_error(VT_ERR_RUNTIME, "There is currently no valid tree for this point cloud");
+  const double* sb = cl->subbox;
+  if ((extent[0] < sb[0]) || (extent[1] > sb[1]) || (extent[2] < sb[2]) || (extent[3] > sb[3]) ||
+      (depth < sb[4]) || (depth > sb[5]))
+    return set_error(VT_ERR_RUNTIME, "Slice extent out of bounds of current cloud subbox");
+  VT_CUDA(cudaSetDevice(cl->device));
+  const double lo[2] = {extent[0], extent[2]};
+  const double step[2] = {(extent[1] - extent[0]) / (double)(npix[0] - 1),
+                          (extent[3] - extent[2]) / (double)(npix[1] - 1)};
+  return grid_sample(cl, false, VT_REDUCE_SUM, npix, lo, step, depth, out);
+  VT_GUARD_END
+}
+
+int vt_brute_projection(vt_cloud* cl, const uint64_t npix[3], const double extent[6], int mode,
+                        double* out) {
+  VT_GUARD_BEGIN
+  if (!cl || !npix || !extent || !out) return set_error(VT_ERR_INVALID, "null argument");
+  // src/brute_projection.cpp:12-32
+  if (mode == VT_REDUCE_VOLUME)
+    return set_error(VT_ERR_INVALID,
+                     "VolumeRender is not supported by BruteProjection: "
+                     "it requires ordered ray segments");
+  if (mode < 0 || mode > 2) return set_error(VT_ERR_INVALID, "Unrecognized reduction mode");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  if (!cl->tree_built)
+    return set_error(VT_ERR_RUNTIME, "There is currently no valid tree for this point cloud");
+  const double* sb = cl->subbox;
+  if ((extent[0] < sb[0]) || (extent[1] > sb[1]) || (extent[2] < sb[2]) || (extent[3] > sb[3]) ||
+      (extent[4] < sb[4]) || (extent[5] > sb[5]))
+    return set_error(VT_ERR_INVALID, "Projection extent out of bounds of current cloud subbox");
+  VT_CUDA(cudaSetDevice(cl->device));
+  const double lo[3] = {extent[0], extent[2], extent[4]};
+  const double step[3] = {(extent[1] - extent[0]) / (double)(npix[0] - 1),
+                          (extent[3] - extent[2]) / (double)(npix[1] - 1),
+                          (extent[5] - extent[4]) / (double)(npix[2] - 1)};
+  return grid_sample(cl, true, mode, npix, lo, step, 0.0, out);
   VT_GUARD_END
 }
 

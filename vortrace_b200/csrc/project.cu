@@ -719,6 +719,89 @@ int run_tape_scatter(vt_cloud* cl, const void* tape, uint64_t n, const double* d
   return VT_OK;
 }
 
+// ------------------------------------------------- slice / brute projection
+// Slice::makeSlice (src/slice.cpp:6-60): pixel (i, j) samples the field of
+// the nearest cell at (x0 + dx i, y0 + dy j, depth); out[(i ny + j) nf + f].
+__global__ void k_slice(DevCloud c, uint64_t nx, uint64_t ny, double x0, double y0, double dx,
+                        double dy, double depth, double* __restrict__ out,
+                        unsigned long long* __restrict__ bad) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nx * ny) return;
+  const uint64_t i = t / ny, j = t % ny;
+  const double qx = dadd(x0, dmul(dx, (double)i));
+  const double qy = dadd(y0, dmul(dy, (double)j));
+  unsigned v = 0;
+  const int cell = nn1_exact64<true>(c, qx, qy, depth, v);
+  if (cell < 0) {
+    atomicMin(bad, (unsigned long long)t);
+    return;
+  }
+  for (int f = 0; f < c.nf; f++) out[t * c.nf + f] = c.fields[(int64_t)cell * c.nf + f];
+}
+
+// BruteProjection::makeProjection (src/brute_projection.cpp:10-96): pixel
+// (i, j) reduces the fields of the nearest cells of the samples
+// (x0 + dx i, y0 + dy j, z0 + dz k), k = 0 .. nz-1 in order; Sum is scaled
+// by dz at the end.
+template <int MODE>
+__global__ void k_brute(DevCloud c, uint64_t nx, uint64_t ny, uint64_t nz, double x0, double y0,
+                        double z0, double dx, double dy, double dz, double* __restrict__ out,
+                        unsigned long long* __restrict__ bad) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nx * ny) return;
+  const uint64_t i = t / ny, j = t % ny;
+  const double qx = dadd(x0, dmul(dx, (double)i));
+  const double qy = dadd(y0, dmul(dy, (double)j));
+  const int nf = c.nf;
+  double* row = out + t * nf;
+  const double init = MODE == kSum ? 0.0 : (MODE == kMax ? -pinf() : pinf());
+  for (int f = 0; f < nf; f++) row[f] = init;
+  for (uint64_t k = 0; k < nz; k++) {
+    const double qz = dadd(z0, dmul(dz, (double)k));
+    unsigned v = 0;
+    const int cell = nn1_exact64<true>(c, qx, qy, qz, v);
+    if (cell < 0) {
+      atomicMin(bad, (unsigned long long)t);
+      return;
+    }
+    for (int f = 0; f < nf; f++) {
+      const double val = c.fields[(int64_t)cell * nf + f];
+      if (MODE == kSum) row[f] = dadd(row[f], val);
+      else if (MODE == kMax) row[f] = val > row[f] ? val : row[f];
+      else row[f] = val < row[f] ? val : row[f];
+    }
+  }
+  if (MODE == kSum)
+    for (int f = 0; f < nf; f++) row[f] = dmul(row[f], dz);
+}
+
+// Launch one of the two; `bad` (device, one slot) receives the first pixel
+// whose query had no finite distance (UINT64_MAX when none).
+int run_grid_sample(vt_cloud* cl, bool brute, int mode, const uint64_t* npix, const double* lo,
+                    const double* step, double depth, double* d_out, unsigned long long* d_bad,
+                    cudaStream_t st) {
+  const uint64_t n = npix[0] * npix[1];
+  if (n == 0) return VT_OK;
+  const int B = 128;
+  const unsigned blocks = (unsigned)((n + B - 1) / B);
+  const DevCloud& c = cl->view;
+  if (!brute) {
+    k_slice<<<blocks, B, 0, st>>>(c, npix[0], npix[1], lo[0], lo[1], step[0], step[1], depth,
+                                  d_out, d_bad);
+  } else if (mode == kSum) {
+    k_brute<kSum><<<blocks, B, 0, st>>>(c, npix[0], npix[1], npix[2], lo[0], lo[1], lo[2],
+                                        step[0], step[1], step[2], d_out, d_bad);
+  } else if (mode == kMax) {
+    k_brute<kMax><<<blocks, B, 0, st>>>(c, npix[0], npix[1], npix[2], lo[0], lo[1], lo[2],
+                                        step[0], step[1], step[2], d_out, d_bad);
+  } else {
+    k_brute<kMin><<<blocks, B, 0, st>>>(c, npix[0], npix[1], npix[2], lo[0], lo[1], lo[2],
+                                        step[0], step[1], step[2], d_out, d_bad);
+  }
+  VT_CUDA(cudaGetLastError());
+  return VT_OK;
+}
+
 int run_knn(vt_cloud* cl, const double* d_q, int64_t nq, int k, int64_t* d_ids, double* d_r2,
             cudaStream_t st) {
   const int B = 128;

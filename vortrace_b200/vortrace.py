@@ -351,3 +351,73 @@ class ProjectionCloud:
         """Exact k nearest generators of query points (original ids, r^2)."""
         ids, r2 = self._cloud.knn(q, k)
         return np.where(ids >= 0, self.orig_ids[np.maximum(ids, 0)], -1), r2
+
+    def slice(self, extent, nres, depth: float) -> np.ndarray:
+        """2D slice at constant depth: the nearest cell's field values at
+        each pixel (vortrace/vortrace.py:347-383; src/slice.cpp:6-60).
+
+        ``extent`` = [xmin, xmax, ymin, ymax]; ``nres``: int or (nx, ny);
+        pixel (i, j) sits at (xmin + i dx, ymin + j dy, depth) with
+        dx = (xmax - xmin) / (nx - 1).  Returns (nx, ny) for one field,
+        else (nx, ny, nfields).
+        """
+        npix = (nres, nres) if isinstance(nres, int) else tuple(nres)
+        extent_arr = np.asarray(extent, dtype=np.float64).ravel()
+        if extent_arr.size != 4:
+            raise ValueError("extent must have 4 elements [xmin, xmax, ymin, ymax]")
+        dat = Slice(list(npix), list(extent_arr), float(depth))
+        dat.makeSlice(self._cloud)
+        out = dat.returnSlice()
+        if self._nfields == 1:
+            return out.reshape(npix[0], npix[1])
+        return out.reshape(npix[0], npix[1], self._nfields)
+
+
+class Slice:
+    """The reference's ``Cvortrace.Slice`` (src/bindings.cpp:259-273)."""
+
+    def __init__(self, npix, extent, depth):
+        self.npix = (int(npix[0]), int(npix[1]))
+        self.extent = np.ascontiguousarray(extent, np.float64).reshape(4)
+        self.depth = float(depth)
+        self._data = None
+
+    def makeSlice(self, cloud: _Cloud):
+        n = self.npix[0] * self.npix[1]
+        nf = int(cloud.info().nfields)
+        out = np.empty((n, nf), np.float64)
+        npx = (C.c_uint64 * 2)(*self.npix)
+        L.check(cloud._lib.vt_slice(cloud._h, npx, L.dptr(self.extent), self.depth,
+                                    L.dptr(out)))
+        self._data = out
+
+    def returnSlice(self):
+        if self._data is None:
+            raise RuntimeError("Slice has not yet been made")
+        return self._data[:, 0].copy() if self._data.shape[1] == 1 else self._data
+
+
+class BruteProjection:
+    """The reference's ``Cvortrace.BruteProjection`` (src/bindings.cpp:240-257):
+    per pixel, the nearest cell's fields summed (times dz), maximised or
+    minimised over a regular grid of depth samples."""
+
+    def __init__(self, npix, extent):
+        self.npix = (int(npix[0]), int(npix[1]), int(npix[2]))
+        self.extent = np.ascontiguousarray(extent, np.float64).reshape(6)
+        self._data = None
+
+    def makeProjection(self, cloud: _Cloud, reduction=L.REDUCE_SUM):
+        mode = _REDUCTIONS[reduction] if isinstance(reduction, str) else int(reduction)
+        n = self.npix[0] * self.npix[1]
+        nf = int(cloud.info().nfields)
+        out = np.empty((n, nf), np.float64)
+        npx = (C.c_uint64 * 3)(*self.npix)
+        L.check(cloud._lib.vt_brute_projection(cloud._h, npx, L.dptr(self.extent), mode,
+                                               L.dptr(out)))
+        self._data = out
+
+    def returnProjection(self):
+        if self._data is None:
+            raise RuntimeError("Projection has not yet been made")
+        return self._data[:, 0].copy() if self._data.shape[1] == 1 else self._data
