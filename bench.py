@@ -263,9 +263,9 @@ def run_ours(args):
                                               d_grad.data_ptr(), stream.cuda_stream))
 
     # forward with a segment tape + scatter adjoint (the autograd path of
-    # 'integrate'); other reductions re-walk the rays in the adjoint
+    # 'integrate' and 'volume')
     tape = L.Tape(lib, h)
-    taped = mode == L.REDUCE_SUM
+    taped = mode in (L.REDUCE_SUM, L.REDUCE_VOLUME)
 
     def fwd_tape():
         if not taped:
@@ -440,8 +440,9 @@ def run_ours(args):
                        "tree_build_ms": round(info.tree_build_ms, 2),
                        "parallelism": f"rays sharded by view, {world} rank(s)"},
             "fwd_bwd_mcrossings_per_s": round(fb_value, 4),
-            "fwd_bwd_adjoint": ("segment tape (16 B/crossing) + scatter" if taped and
-                                tape_entries > 0 else "re-walk"),
+            "fwd_bwd_adjoint": (f"segment tape ({48 if mode == L.REDUCE_VOLUME else 16} "
+                                "B/crossing) + scatter" if taped and tape_entries > 0
+                                else "re-walk"),
             "fwd_bwd_rewalk_mcrossings_per_s": round(rw_value, 4),
             "kernel": "batched (VT_KERNEL_AUTO = VT_KERNEL_THREAD_FP32)",
             "bounded_fp64_mcrossings_per_s": round(f64_value, 4),

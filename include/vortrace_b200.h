@@ -225,11 +225,13 @@ int vt_brute_projection(vt_cloud *cloud, const uint64_t npix[3], const double ex
                         int mode, double *out);
 
 /* Segment tape (no reference counterpart; the reference has no gradients).
- * vt_project_device_tape is vt_project_device for SUM that also records, in
- * device memory owned by the tape, one (cell, ray, ds) entry per segment --
- * 16 bytes per crossing (3.2 GB for 2e8 crossings).  vt_tape_adjoint_device
- * then computes the SUM adjoint as a scatter of those entries instead of a
- * second walk.  The tape grows to the entries the last forward on it
+ * vt_project_device_tape is vt_project_device for SUM or VOLUME that also
+ * records, in device memory owned by the tape, one entry per segment: (cell,
+ * ray, ds), 16 bytes per crossing (3.2 GB for 2e8 crossings), for SUM; also
+ * the transmittance in front of the segment and the colour composited up to
+ * it, 48 bytes per crossing, for VOLUME.  vt_tape_adjoint_device then
+ * computes the adjoint as a scatter of those entries instead of a second
+ * walk.  The tape grows to the entries the last forward on it
  * needed; a forward whose segments did not fit leaves the tape invalid, and
  * the adjoint of an invalid or mismatched tape (other cloud, ray count or
  * mode) re-walks the rays like vt_project_adjoint_device, so the result is

@@ -9,8 +9,9 @@ backward is the hand-written adjoint kernel (vt_project_adjoint_device):
   backward is a scatter of it (vt_tape_adjoint_device); a tape that did not
   fit falls back to re-walking the rays;
 * ``'volume'``: reverse-mode front-to-back compositing; the transmittance in
-  front of every segment and the light behind it are recomputed by re-walking
-  the ray (no per-ray segment lists are stored).
+  front of every segment and the colour composited up to it come from the
+  forward's tape (48 bytes per crossing), or are recomputed by re-walking the
+  ray when the tape did not fit.
 
 The cell geometry does not depend on the fields, so the segment lists are
 the same in the forward and the backward walk.  PyTorch is only the autograd
@@ -57,7 +58,7 @@ class _ProjectFn(torch.autograd.Function):
         out = torch.empty((n, nout), dtype=torch.float64, device=dev)
         st = L.Stats()
         tape = None
-        if mode == L.REDUCE_SUM and ctx.needs_input_grad[0]:
+        if mode in (L.REDUCE_SUM, L.REDUCE_VOLUME) and ctx.needs_input_grad[0]:
             tape = _take_tape(pc)
             L.check(lib.vt_project_device_tape(h, tape.h, _dev_ptr(starts), _dev_ptr(ends), n,
                                                mode, kernel, _dev_ptr(out), stream,

@@ -24,6 +24,8 @@ int scan_offsets(vt_cloud* cl, const int64_t* d_counts, int64_t* d_offsets, int6
                  cudaStream_t st);
 int run_tape_scatter(vt_cloud* cl, const void* tape, uint64_t n, const double* d_gout,
                      double* d_grad, cudaStream_t st);
+int run_tape_scatter_vol(vt_cloud* cl, const void* tape, uint64_t n, const double* d_gout,
+                         const double* d_fwd, double* d_grad, cudaStream_t st);
 int run_grid_sample(vt_cloud* cl, bool brute, int mode, const uint64_t* npix, const double* lo,
                     const double* step, double depth, double* d_out, unsigned long long* d_bad,
                     cudaStream_t st);
@@ -682,7 +684,8 @@ int vt_project_device_tape(vt_cloud* cl, vt_tape* tape, const double* d_starts,
   int rc = check_projectable(cl, mode);
   if (rc) return rc;
   if (!tape) return set_error(VT_ERR_INVALID, "null tape handle");
-  if (mode != VT_REDUCE_SUM) return set_error(VT_ERR_INVALID, "a tape is recorded for 'integrate' only");
+  if (mode != VT_REDUCE_SUM && mode != VT_REDUCE_VOLUME)
+    return set_error(VT_ERR_INVALID, "a tape is recorded for 'integrate' and 'volume' only");
   if (nrays > (uint64_t)std::numeric_limits<int32_t>::max())
     return set_error(VT_ERR_INVALID, "a taped projection takes at most 2^31-1 rays");
   std::lock_guard<std::mutex> lk(cl->mu);
@@ -692,7 +695,9 @@ int vt_project_device_tape(vt_cloud* cl, vt_tape* tape, const double* d_starts,
   tape->n = 0;
   tape->nrays = nrays;
   tape->nfields = cl->nfields;
+  tape->mode = mode;
   tape->cloud = cl;
+  const size_t esize = mode == VT_REDUCE_VOLUME ? sizeof(vt::TapeEntryV) : sizeof(vt::TapeEntry);
   if (nrays == 0) {
     tape->valid = true;
     return VT_OK;
@@ -703,10 +708,10 @@ int vt_project_device_tape(vt_cloud* cl, vt_tape* tape, const double* d_starts,
   uint64_t need = tape->want;
   if (cl->cross_per_ray > 0.0)
     need = std::max<uint64_t>(need, (uint64_t)(1.25 * cl->cross_per_ray * (double)nrays) + 1024);
-  if (need > tape->cap) {
-    if ((rc = tape->buf.reserve(need * sizeof(vt::TapeEntry)))) return rc;
-    tape->cap = need;
+  if (need * esize > tape->buf.bytes()) {
+    if ((rc = tape->buf.reserve(need * esize))) return rc;
   }
+  tape->cap = tape->buf.bytes() / esize;
   if ((rc = tape->count.reserve(1))) return rc;
   cudaStream_t st = pick_stream(cl, stream);
   VT_CUDA(cudaMemsetAsync(tape->count.p, 0, sizeof(unsigned long long), st));
@@ -714,9 +719,9 @@ int vt_project_device_tape(vt_cloud* cl, vt_tape* tape, const double* d_starts,
   io.starts = d_starts;
   io.ends = d_ends;
   io.nrays = (int64_t)nrays;
-  io.nout = (int)cl->nfields;
+  io.nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
   io.out = d_out;
-  io.tape = reinterpret_cast<vt::TapeEntry*>(tape->buf.p);
+  io.tape = tape->buf.p;
   io.tape_count = tape->count.p;
   io.tape_cap = tape->cap;
   // the warp-per-ray kernel keeps no tape: AUTO and BATCHED run one ray per thread
@@ -748,9 +753,13 @@ int vt_tape_adjoint_device(vt_cloud* cl, vt_tape* tape, const double* d_starts,
   VT_CUDA(cudaSetDevice(cl->device));
   if (nrays == 0) return VT_OK;
   cudaStream_t st = pick_stream(cl, stream);
-  if (mode == VT_REDUCE_SUM && tape->valid && tape->cloud == cl && tape->nrays == nrays &&
-      tape->nfields == cl->nfields)
+  if (tape->valid && tape->mode == mode && tape->cloud == cl && tape->nrays == nrays &&
+      tape->nfields == cl->nfields) {
+    if (mode == VT_REDUCE_VOLUME)
+      return vt::run_tape_scatter_vol(cl, tape->buf.p, tape->n, d_grad_out, d_out,
+                                      d_grad_fields, st);
     return vt::run_tape_scatter(cl, tape->buf.p, tape->n, d_grad_out, d_grad_fields, st);
+  }
   return adjoint_locked(cl, d_starts, d_ends, nrays, mode, d_out, d_grad_out, d_grad_fields, st);
   VT_GUARD_END
 }

@@ -127,18 +127,20 @@ struct vt_cloud {
   vt::DevBuf<uint8_t> ws_order;  // ray sort keys, order and CUB scratch
 };
 
-// Segment tape of one 'integrate' forward (vt_project_device_tape): the
-// entries (cell, ray, ds) of every segment, in no particular order, so that
-// the adjoint is a scatter instead of a second walk.
+// Segment tape of one 'integrate' or 'volume' forward
+// (vt_project_device_tape): one entry per segment (TapeEntry / TapeEntryV),
+// in no particular order, so that the adjoint is a scatter instead of a
+// second walk.
 struct vt_tape {
   int device = 0;
-  vt::DevBuf<uint8_t> buf;                 // TapeEntry[cap]
+  vt::DevBuf<uint8_t> buf;                 // cap entries
   vt::DevBuf<unsigned long long> count;    // entries appended by the last forward
   uint64_t cap = 0;     // entries buf holds
   uint64_t n = 0;       // entries recorded by the last forward
   uint64_t want = 0;    // entries the last forward needed
   uint64_t nrays = 0;   // rays of the last forward
   uint64_t nfields = 0;
+  int mode = 0;         // reduction of the last forward (SUM or VOLUME)
   const vt_cloud* cloud = nullptr;
   bool valid = false;   // the last forward recorded every segment
 };

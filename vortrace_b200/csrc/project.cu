@@ -105,7 +105,8 @@ struct Reducer {
 // Append one tape entry; the lanes of a warp that reach this point together
 // reserve their slots with one atomic.  Entries past tape_cap are counted
 // but not written (the host then sizes the tape from the count).
-__device__ __forceinline__ void tape_append(const WalkIO& io, int pid, int ray, double ds) {
+template <class E>
+__device__ __forceinline__ void tape_append(const WalkIO& io, const E& e) {
   const unsigned m = __activemask();
   const int lane = threadIdx.x & 31;
   const int leader = __ffs(m) - 1;
@@ -113,11 +114,11 @@ __device__ __forceinline__ void tape_append(const WalkIO& io, int pid, int ray, 
   if (lane == leader) base = atomicAdd(io.tape_count, (unsigned long long)__popc(m));
   base = __shfl_sync(m, base, leader);
   const unsigned long long k = base + __popc(m & ((1u << lane) - 1u));
-  if (k < io.tape_cap) io.tape[k] = TapeEntry{pid, ray, ds};
+  if (k < io.tape_cap) static_cast<E*>(io.tape)[k] = e;
 }
 
-// Reducer of 'integrate' that also records the tape; the first `skip`
-// segments of the ray were recorded by an earlier, handed-over launch.
+// Reducer of 'integrate' or 'volume' that also records the tape; the first
+// `skip` segments of the ray were recorded by an earlier, handed-over launch.
 template <int MODE, int NF>
 struct TapeReducer : Reducer<MODE, NF> {
   const WalkIO* io;
@@ -129,8 +130,16 @@ struct TapeReducer : Reducer<MODE, NF> {
     skip = sk;
   }
   __device__ __forceinline__ void seg(int cell, double a, double b) {
-    Reducer<MODE, NF>::seg(cell, a, b);
-    if (this->nseg > skip) tape_append(*io, this->c->perm[cell], ray, dsub(b, a));
+    if (MODE == kVolume) {
+      const double T0 = this->T;
+      Reducer<MODE, NF>::seg(cell, a, b);
+      if (this->nseg > skip)
+        tape_append(*io, TapeEntryV{cell, ray, dsub(b, a), T0,
+                                    {this->acc[0], this->acc[1], this->acc[2]}});
+    } else {
+      Reducer<MODE, NF>::seg(cell, a, b);
+      if (this->nseg > skip) tape_append(*io, TapeEntry{this->c->perm[cell], ray, dsub(b, a)});
+    }
   }
 };
 
@@ -471,8 +480,10 @@ static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int ker
     case kOutCount: rc = launch_walk_mode<kOutCount>(cl, io, mode, kernel, st); break;
     case kOutFill: rc = launch_walk_t<kSum, 1, kOutFill>(cl, io, kernel, st); break;
     case kOutTape:
-      if (mode != kSum) return set_error(VT_ERR_INVALID, "a tape is recorded for 'integrate' only");
-      if (cl->nfields == 1) rc = launch_walk_t<kSum, 1, kOutTape>(cl, io, kernel, st);
+      if (mode != kSum && mode != kVolume)
+        return set_error(VT_ERR_INVALID, "a tape is recorded for 'integrate' and 'volume' only");
+      if (mode == kVolume) rc = launch_walk_t<kVolume, 4, kOutTape>(cl, io, kernel, st);
+      else if (cl->nfields == 1) rc = launch_walk_t<kSum, 1, kOutTape>(cl, io, kernel, st);
       else if (cl->nfields == 3) rc = launch_walk_t<kSum, 3, kOutTape>(cl, io, kernel, st);
       else if (cl->nfields == 4) rc = launch_walk_t<kSum, 4, kOutTape>(cl, io, kernel, st);
       else rc = launch_walk_t<kSum, 0, kOutTape>(cl, io, kernel, st);
@@ -699,6 +710,65 @@ __global__ void k_tape_scatter(const TapeEntry* __restrict__ t, uint64_t n, int 
       if (leader && pid >= 0) atomicAdd(&grad[(int64_t)pid * nf + f], sum);
     }
   }
+}
+
+// Adjoint of 'volume' from a tape (the formulas of AdjSink): with
+// e = exp(-alpha ds), o = 1 - e, T and P of the entry and C the ray's final
+// colour, grad[rgb_k] += g_k T o and grad[alpha] += ds sum_k g_k (T rgb_k e -
+// (C_k - P_k)); lanes holding the same cell add their terms first.
+__global__ void k_tape_scatter_vol(DevCloud c, const TapeEntryV* __restrict__ t, uint64_t n,
+                                   const double* __restrict__ gout,
+                                   const double* __restrict__ fwd, double* __restrict__ grad) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const uint64_t i = base + threadIdx.x;
+    int pid = -1;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (i < n) {
+      const TapeEntryV e = t[i];
+      pid = c.perm[e.cell];
+      const double* F = c.fields + (int64_t)e.cell * 4;
+      const double ex = exp(dmul(-F[3], e.ds));
+      const double o = dsub(1.0, ex);
+      double galpha = 0.0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double g = gout[(int64_t)e.ray * 3 + k];
+        const double S = fwd[(int64_t)e.ray * 3 + k] - e.P[k];
+        galpha += g * (e.T * F[k] * ex - S);
+        v[k] = g * e.T * o;
+      }
+      v[3] = e.ds * galpha;
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, pid);
+    const bool leader = __ffs(peers) - 1 == lane;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      double sum = 0.0;
+#pragma unroll 8
+      for (int j = 0; j < 32; ++j) {
+        const double vj = __shfl_sync(0xffffffffu, v[f], j);
+        if ((peers >> j) & 1u) sum += vj;
+      }
+      if (leader && pid >= 0) atomicAdd(&grad[(int64_t)pid * 4 + f], sum);
+    }
+  }
+}
+
+int run_tape_scatter_vol(vt_cloud* cl, const void* tape, uint64_t n, const double* d_gout,
+                         const double* d_fwd, double* d_grad, cudaStream_t st) {
+  if (n == 0) return VT_OK;
+  int dev = 0, nsms = 0;
+  VT_CUDA(cudaGetDevice(&dev));
+  VT_CUDA(cudaDeviceGetAttribute(&nsms, cudaDevAttrMultiProcessorCount, dev));
+  const int B = 256;
+  uint64_t blocks = (n + B - 1) / B;
+  if (blocks > (uint64_t)nsms * 16) blocks = (uint64_t)nsms * 16;
+  k_tape_scatter_vol<<<(unsigned)blocks, B, 0, st>>>(
+      cl->view, static_cast<const TapeEntryV*>(tape), n, d_gout, d_fwd, d_grad);
+  VT_CUDA(cudaGetLastError());
+  return VT_OK;
 }
 
 int run_tape_scatter(vt_cloud* cl, const void* tape, uint64_t n, const double* d_gout,

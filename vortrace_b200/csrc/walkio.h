@@ -11,7 +11,7 @@ struct vt_cloud;
 
 namespace vt {
 
-// kOutTape: the image of 'integrate' plus one tape entry per segment
+// kOutTape: the image of 'integrate' or 'volume' plus one tape entry per segment
 constexpr int kOutImage = 0, kOutCount = 1, kOutFill = 2, kOutAdj = 3, kOutTape = 4;
 
 // One segment of a taped forward: the adjoint of 'integrate' needs only
@@ -20,6 +20,17 @@ struct TapeEntry {
   int32_t pid;
   int32_t ray;
   double ds;
+};
+// One segment of a taped 'volume' forward: the cell (tree index), the ray,
+// the segment length, the transmittance in front of the segment and the
+// composited colour up to and including it -- what the reverse-mode
+// compositing adjoint needs besides the fields and the final colour.
+struct TapeEntryV {
+  int32_t cell;
+  int32_t ray;
+  double ds;
+  double T;
+  double P[3];
 };
 constexpr int kErrNonFinite = 16;
 
@@ -49,7 +60,7 @@ struct WalkIO {
   int local_cap;         // in-register stack entries per ray
   int cache_mode;        // batched kernel: 1 = neighbourhood cache on
   const int32_t* order;  // batched kernels: ray visiting order (NULL: 0..nrays-1)
-  TapeEntry* tape;       // kOutTape: entries [0, tape_cap) of the tape
+  void* tape;            // kOutTape: entries [0, tape_cap) (TapeEntry, or TapeEntryV for volume)
   unsigned long long* tape_count;  // kOutTape: entries appended (may exceed tape_cap)
   unsigned long long tape_cap;
   WalkDiag* diag;
