@@ -365,6 +365,17 @@ def run_ours(args):
     t_f64 = reduce_max(sum(f64_ms))
     f64_value = tot_cross * kp / (t_f64 / 1e3) / 1e6
 
+    # --- the plain kernel's own forward + adjoint (re-walk, plain kernel)
+    pc._cloud.set_param(L.PARAM_ADJOINT_KERNEL, L.KERNEL_PLAIN_FP64)
+    fwd(L.KERNEL_PLAIN_FP64)
+    bwd()
+    barrier()
+    pfb_ms = timed(lambda: (fwd(L.KERNEL_PLAIN_FP64), bwd()), kp)
+    barrier()
+    pc._cloud.set_param(L.PARAM_ADJOINT_KERNEL, L.KERNEL_AUTO)
+    t_pfb = reduce_max(sum(pfb_ms))
+    pfb_value = tot_cross * kp / (t_pfb / 1e3) / 1e6
+
     # --- plain FP64 one-ray-per-thread kernel (the baseline kernel)
     fwd(L.KERNEL_PLAIN_FP64)
     barrier()
@@ -448,6 +459,8 @@ def run_ours(args):
             "bounded_fp64_mcrossings_per_s": round(f64_value, 4),
             "plain_fp64_mcrossings_per_s": round(pl_value, 4),
             "speedup_vs_plain_fp64": round(value / pl_value, 3),
+            "plain_fp64_fwd_bwd_mcrossings_per_s": round(pfb_value, 4),
+            "fwd_bwd_speedup_vs_plain_fp64_fwd_bwd": round(fb_value / pfb_value, 3),
             "rays_per_s": round(n * world * K / (t_fwd / 1e3), 1),
             "fp64_resolve_fraction": round(resolves / max(1, queries), 6),
             "e2e": {"value": round(e2e_value, 4), "unit": UNIT,

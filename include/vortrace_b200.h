@@ -75,10 +75,13 @@ extern "C" {
                                   /* (default and maximum: the compiled size)  */
 #define VT_PARAM_CACHE 8          /* batched kernel: per-ray neighbourhood     */
                                   /* cache of the split-point queries (1, 0)   */
+#define VT_PARAM_ADJOINT_KERNEL 9 /* walk kernel of the re-walk adjoint        */
+                                  /* (VT_KERNEL_*; default AUTO)               */
 
 typedef struct vt_cloud vt_cloud;
 typedef struct vt_segments vt_segments;
 typedef struct vt_tape vt_tape;
+typedef struct vt_graph vt_graph;
 
 typedef struct {
   uint64_t npart;      /* points after filtering (PointCloud::get_npart)   */
@@ -210,6 +213,42 @@ int vt_project_adjoint(vt_cloud *cloud, const double *starts, const double *ends
 int vt_project_adjoint_device(vt_cloud *cloud, const double *d_starts, const double *d_ends,
                               uint64_t nrays, int mode, const double *d_out,
                               const double *d_grad_out, double *d_grad_fields, void *stream);
+
+/* CUDA graph of a forward projection (no reference counterpart): the
+ * counter resets, the ray sort, the walk kernel and the global-stack kernel
+ * for fixed device buffers (d_starts, d_ends: nrays x 3; d_out: nrays x nout)
+ * captured once; vt_graph_launch replays them on `stream` with one
+ * cudaGraphLaunch, reading the rays the buffers hold at that time.
+ * vt_graph_finish waits for `stream`, returns the counters and reports a
+ * failed ray like vt_project_device.  The graph owns its scratch; rebuilding
+ * the cloud's tree or reallocating its fields invalidates it (launch then
+ * fails).  Launches of one graph must not overlap. */
+int vt_graph_create(vt_cloud *cloud, const double *d_starts, const double *d_ends,
+                    uint64_t nrays, int mode, int kernel, double *d_out, vt_graph **out);
+int vt_graph_launch(vt_graph *graph, void *stream);
+int vt_graph_finish(vt_graph *graph, void *stream, vt_stats *stats);
+void vt_graph_destroy(vt_graph *graph);
+
+/* Autotuner (no reference counterpart).  Times the walk kernels (one ray
+ * per thread with the guarded-FP32 or the FP64 search, one ray per warp) and
+ * the number of tree levels staged in shared memory (0-9) on a sample of
+ * the given rays (host arrays, nrays x 3) -- up to max_sample (0: 65,536)
+ * rays in four contiguous
+ * blocks, each configuration run twice, the second run timed -- and makes
+ * the fastest the cloud's VT_KERNEL_AUTO choice for batches at least as
+ * large as the sample (VT_PARAM_SMEM_LEVELS is set to its value).  Results
+ * of every kernel are the same bits; only the speed changes. */
+typedef struct {
+  int32_t kernel;           /* chosen VT_KERNEL_*                            */
+  int32_t smem_levels;      /* chosen tree levels in shared memory           */
+  int32_t tried;            /* configurations timed                          */
+  int32_t pad;
+  uint64_t sample_rays;     /* rays in the sample                            */
+  double mcrossings_per_s;  /* the chosen configuration on the sample        */
+} vt_tune_result;
+int vt_cloud_autotune(vt_cloud *cloud, const double *starts, const double *ends,
+                      uint64_t nrays, int mode, uint64_t max_sample,
+                      vt_tune_result *result);
 
 /* Slice::makeSlice (src/slice.cpp:6-60, src/bindings.cpp:259-273): out[(i *
  * npix[1] + j) * nfields + f] = field f of the cell nearest to (extent[0] +

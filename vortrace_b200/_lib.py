@@ -33,6 +33,7 @@ PARAM_BLOCKS_PER_SM = 5
 PARAM_LEAF_SIZE = 6
 PARAM_LOCAL_STACK = 7
 PARAM_CACHE = 8
+PARAM_ADJOINT_KERNEL = 9
 
 # every symbol the header declares (checked by the tests)
 EXPORTS = (
@@ -44,7 +45,8 @@ EXPORTS = (
     "vt_segments_count",
     "vt_segments_copy", "vt_segments_free", "vt_project_adjoint", "vt_project_adjoint_device",
     "vt_tape_create", "vt_tape_destroy", "vt_tape_size", "vt_project_device_tape",
-    "vt_tape_adjoint_device", "vt_slice", "vt_brute_projection",
+    "vt_tape_adjoint_device", "vt_slice", "vt_brute_projection", "vt_cloud_autotune",
+    "vt_graph_create", "vt_graph_launch", "vt_graph_finish", "vt_graph_destroy",
 )
 
 
@@ -54,6 +56,17 @@ class CloudInfo(C.Structure):
                 ("tree_built", C.c_int32), ("periodic", C.c_int32), ("tree_depth", C.c_int32),
                 ("tree_leaves", C.c_uint64), ("tree_build_ms", C.c_double),
                 ("device_bytes", C.c_uint64)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("kernel", C.c_int32), ("smem_levels", C.c_int32), ("tried", C.c_int32),
+                ("pad", C.c_int32), ("sample_rays", C.c_uint64), ("mcrossings_per_s", C.c_double)]
+
+    def as_dict(self):
+        names = {v: k for k, v in KERNELS.items()}
+        return {"kernel": names.get(self.kernel, self.kernel), "smem_levels": self.smem_levels,
+                "tried": self.tried, "sample_rays": self.sample_rays,
+                "mcrossings_per_s": self.mcrossings_per_s}
 
 
 class Stats(C.Structure):
@@ -130,6 +143,12 @@ def load(path: str | None = None):
         L.vt_tape_destroy.argtypes = [vp]
         L.vt_tape_destroy.restype = None
         L.vt_slice.argtypes = [vp, C.POINTER(u64), dp, C.c_double, dp]
+        L.vt_cloud_autotune.argtypes = [vp, dp, dp, u64, C.c_int, u64, C.POINTER(TuneResult)]
+        L.vt_graph_create.argtypes = [vp, vp, vp, u64, C.c_int, C.c_int, vp, C.POINTER(vp)]
+        L.vt_graph_launch.argtypes = [vp, vp]
+        L.vt_graph_finish.argtypes = [vp, vp, C.POINTER(Stats)]
+        L.vt_graph_destroy.argtypes = [vp]
+        L.vt_graph_destroy.restype = None
         L.vt_brute_projection.argtypes = [vp, C.POINTER(u64), dp, C.c_int, dp]
         L.vt_tape_size.argtypes = [vp]
         L.vt_tape_size.restype = u64
@@ -143,7 +162,8 @@ def load(path: str | None = None):
                      "vt_segments_copy",
                      "vt_project_adjoint", "vt_project_adjoint_device", "vt_set_device",
                      "vt_tape_create", "vt_project_device_tape", "vt_tape_adjoint_device",
-                     "vt_slice", "vt_brute_projection"):
+                     "vt_slice", "vt_brute_projection", "vt_cloud_autotune",
+                     "vt_graph_create", "vt_graph_launch", "vt_graph_finish"):
             getattr(L, name).restype = C.c_int
         L.vt_set_warning_callback(_warn_cb)
         _lib = L

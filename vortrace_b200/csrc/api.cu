@@ -54,6 +54,7 @@ bool verbose() { return g_verbose.load(); }
 }  // namespace vt
 
 using vt::check_projectable;
+using vt::resolve_kernel;
 using vt::set_error;
 
 #define VT_GUARD_BEGIN try {
@@ -87,11 +88,13 @@ int vt::check_projectable(const vt_cloud* cl, int mode) {
 // of the device's SMs to hide its memory latency; batches smaller than
 // kThreadKernelMinRays cannot fill the device that way and run one ray per
 // warp instead (measured on B200: 16,384 rays, 1.4x faster per warp).
+// vt_cloud_autotune replaces the rule by its measured choice for batches of
+// at least its sample's size.
 constexpr uint64_t kThreadKernelMinRays = 65536;
-static int resolve_kernel(int kernel, uint64_t nrays) {
-  if (kernel == VT_KERNEL_AUTO)
-    return nrays < kThreadKernelMinRays ? VT_KERNEL_BATCHED : VT_KERNEL_THREAD_FP32;
-  return kernel;
+int vt::resolve_kernel(const vt_cloud* cl, int kernel, uint64_t nrays) {
+  if (kernel != VT_KERNEL_AUTO) return kernel;
+  if (cl->tuned_kernel != VT_KERNEL_AUTO && nrays >= cl->tuned_min_rays) return cl->tuned_kernel;
+  return nrays < kThreadKernelMinRays ? VT_KERNEL_BATCHED : VT_KERNEL_THREAD_FP32;
 }
 
 static cudaStream_t pick_stream(vt_cloud* cl, void* s) {
@@ -315,6 +318,11 @@ int vt_cloud_set_param(vt_cloud* cl, int param, int64_t value) {
       if (value < 0 || value > 1) return set_error(VT_ERR_INVALID, "cache mode must be 0 or 1");
       cl->cache_mode = (int)value;
       return VT_OK;
+    case VT_PARAM_ADJOINT_KERNEL:
+      if (value < VT_KERNEL_AUTO || value > VT_KERNEL_THREAD_FP32)
+        return set_error(VT_ERR_INVALID, "unknown kernel");
+      cl->adjoint_kernel = (int)value;
+      return VT_OK;
     case VT_PARAM_LEAF_SIZE:
       if (value < 2 || value > 64) return set_error(VT_ERR_INVALID, "leaf size out of range [2, 64]");
       cl->leaf_size = (int)value;
@@ -408,7 +416,7 @@ static int project_device_locked(vt_cloud* cl, const double* d_starts, const dou
   io.nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
   io.out = d_out;
   io.counts = d_counts;
-  return vt::run_walk(cl, io, out_kind, mode, resolve_kernel(kernel, io.nrays), st, stats);
+  return vt::run_walk(cl, io, out_kind, mode, resolve_kernel(cl, kernel, io.nrays), st, stats);
 }
 
 int vt_project_device(vt_cloud* cl, const double* d_starts, const double* d_ends,
@@ -563,7 +571,7 @@ static int adjoint_locked(vt_cloud* cl, const double* d_starts, const double* d_
   io.gout = d_gout;
   io.fwd = d_out;
   io.grad = d_grad;
-  return vt::run_walk(cl, io, vt::kOutAdj, mode, resolve_kernel(VT_KERNEL_AUTO, nrays), st,
+  return vt::run_walk(cl, io, vt::kOutAdj, mode, resolve_kernel(cl, cl->adjoint_kernel, nrays), st,
                       nullptr);
 }
 
@@ -657,6 +665,82 @@ int vt_brute_projection(vt_cloud* cl, const uint64_t npix[3], const double exten
   VT_GUARD_END
 }
 
+int vt_cloud_autotune(vt_cloud* cl, const double* starts, const double* ends, uint64_t nrays,
+                      int mode, uint64_t max_sample, vt_tune_result* result) {
+  VT_GUARD_BEGIN
+  int rc = check_projectable(cl, mode);
+  if (rc) return rc;
+  if (!result) return set_error(VT_ERR_INVALID, "result must not be NULL");
+  memset(result, 0, sizeof(*result));
+  std::lock_guard<std::mutex> lk(cl->mu);
+  VT_CUDA(cudaSetDevice(cl->device));
+  if (nrays == 0) return set_error(VT_ERR_INVALID, "autotune needs at least one ray");
+  if (max_sample == 0) max_sample = 65536;
+  const uint64_t m = nrays < max_sample ? nrays : max_sample;
+  if (!starts || !ends) return set_error(VT_ERR_INVALID, "starts/ends must not be NULL");
+  cudaStream_t st = cl->stream;
+  // sample: four contiguous blocks (neighbouring rays stay neighbours)
+  vt::DevBuf<double> ss, se, so;
+  const int nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
+  if ((rc = ss.alloc(3 * m)) || (rc = se.alloc(3 * m)) || (rc = so.alloc(m * nout))) return rc;
+  uint64_t done = 0;
+  for (int b = 0; b < 4; ++b) {
+    const uint64_t len = (m * (b + 1)) / 4 - done;
+    const uint64_t at = (nrays * (2 * b + 1)) / 8 > len / 2 ? (nrays * (2 * b + 1)) / 8 - len / 2 : 0;
+    const uint64_t from = at + len <= nrays ? at : nrays - len;
+    VT_CUDA(cudaMemcpyAsync(ss.p + 3 * done, starts + 3 * from, 3 * len * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+    VT_CUDA(cudaMemcpyAsync(se.p + 3 * done, ends + 3 * from, 3 * len * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+    done += len;
+  }
+  struct Cand {
+    int kernel, smem;
+  };
+  const Cand cands[] = {{VT_KERNEL_THREAD_FP32, 0}, {VT_KERNEL_THREAD_FP32, 3},
+                        {VT_KERNEL_THREAD_FP32, 5}, {VT_KERNEL_THREAD_FP32, 7},
+                        {VT_KERNEL_THREAD_FP32, 9}, {VT_KERNEL_BATCHED_FP64, 0},
+                        {VT_KERNEL_BATCHED_FP64, 5}, {VT_KERNEL_BATCHED, 5}};
+  const int saved_smem = cl->smem_levels;
+  double best_ms = -1.0;
+  Cand best = cands[0];
+  uint64_t crossings = 0;
+  for (const Cand& cd : cands) {
+    if (cl->periodic && cd.kernel != VT_KERNEL_THREAD_FP32) continue;  // one kernel serves them
+    cl->smem_levels = cd.smem;
+    double ms = 0.0;
+    for (int rep = 0; rep < 2; ++rep) {  // the first run warms the caches
+      vt::WalkIO io{};
+      io.starts = ss.p;
+      io.ends = se.p;
+      io.nrays = (int64_t)m;
+      io.nout = nout;
+      io.out = so.p;
+      vt_stats sts;
+      if ((rc = vt::run_walk(cl, io, vt::kOutImage, mode, cd.kernel, st, &sts))) {
+        cl->smem_levels = saved_smem;
+        return rc;
+      }
+      ms = sts.walk_ms;
+      crossings = sts.crossings;
+    }
+    ++result->tried;
+    if (best_ms < 0.0 || ms < best_ms) {
+      best_ms = ms;
+      best = cd;
+    }
+  }
+  cl->smem_levels = best.smem;
+  cl->tuned_kernel = best.kernel;
+  cl->tuned_min_rays = m;
+  result->kernel = best.kernel;
+  result->smem_levels = best.smem;
+  result->sample_rays = m;
+  result->mcrossings_per_s = best_ms > 0.0 ? (double)crossings / (best_ms * 1e3) : 0.0;
+  return VT_OK;
+  VT_GUARD_END
+}
+
 int vt_tape_create(vt_cloud* cl, vt_tape** out) {
   VT_GUARD_BEGIN
   if (!out) return set_error(VT_ERR_INVALID, "out must not be NULL");
@@ -725,7 +809,7 @@ int vt_project_device_tape(vt_cloud* cl, vt_tape* tape, const double* d_starts,
   io.tape_count = tape->count.p;
   io.tape_cap = tape->cap;
   // the warp-per-ray kernel keeps no tape: AUTO and BATCHED run one ray per thread
-  int k = resolve_kernel(kernel, nrays);
+  int k = resolve_kernel(cl, kernel, nrays);
   if (k == VT_KERNEL_BATCHED) k = VT_KERNEL_THREAD_FP32;
   if ((rc = vt::run_walk(cl, io, vt::kOutTape, mode, k, st, stats))) return rc;
   unsigned long long used = 0;

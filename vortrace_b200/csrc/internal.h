@@ -105,6 +105,9 @@ struct vt_cloud {
   int blocks_per_sm = 0;
   int local_stack = 1 << 30;  // capped to the compiled size in the kernels
   int cache_mode = 0;
+  int adjoint_kernel = VT_KERNEL_AUTO;  // kernel of the re-walk adjoint
+  int tuned_kernel = VT_KERNEL_AUTO;    // vt_cloud_autotune's choice for AUTO
+  uint64_t tuned_min_rays = 0;          // ... for batches at least this large
   // device tree (tree order)
   vt::DevBuf<double4> pts_d;
   vt::DevBuf<float4> pts32_d;
@@ -150,4 +153,6 @@ int build_tree_device(vt_cloud* cl);
 int upload_fields(vt_cloud* cl, const double* src, bool src_device, cudaStream_t st);
 // tree built, mode valid, volume needs valid RGBA (src/reduction.cpp:59-66)
 int check_projectable(const vt_cloud* cl, int mode);
+// the kernel VT_KERNEL_AUTO stands for with this cloud and batch size
+int resolve_kernel(const vt_cloud* cl, int kernel, uint64_t nrays);
 }

@@ -21,6 +21,7 @@
 
 #include <chrono>
 #include <cstdio>
+#include <memory>
 #include <type_traits>
 
 #include "internal.h"
@@ -449,13 +450,10 @@ static std::string fmt_double(double v) {
   return buf;
 }
 
-// One walk launch (+ handed-over rays) on scratch already placed in `io`
-// (stats, hand-over queue, global stacks); turns a per-ray failure into the
-// reference's error message.  `d_diag`: device scratch for the diagnosis of
-// a failing ray (NULL: allocated on demand).  `timed`: CUDA events around
-// the launches for vt_stats.walk_ms.
-static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel,
-                       cudaStream_t st, vt_stats* stats, WalkDiag* d_diag, bool timed) {
+// Enqueue one walk on `st`: counters reset, then the kernels.  No host
+// synchronisation, so the sequence can be captured into a CUDA graph.
+static int enqueue_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel,
+                        cudaStream_t st) {
   // periodic clouds: the periodic k-NN merge and minimum-image split points
   // live in the exact FP64 walk of the one-ray-per-thread kernel
   if (cl->periodic) {
@@ -468,28 +466,39 @@ static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int ker
   io.diag = nullptr;
   VT_CUDA(cudaMemsetAsync(io.stats, 0, sizeof(DevStats), st));
   VT_CUDA(cudaMemsetAsync(&io.stats->first_error, 0xff, sizeof(unsigned long long), st));
+  switch (out_kind) {
+    case kOutImage: return launch_walk_mode<kOutImage>(cl, io, mode, kernel, st);
+    case kOutCount: return launch_walk_mode<kOutCount>(cl, io, mode, kernel, st);
+    case kOutFill: return launch_walk_t<kSum, 1, kOutFill>(cl, io, kernel, st);
+    case kOutTape:
+      if (mode != kSum && mode != kVolume)
+        return set_error(VT_ERR_INVALID, "a tape is recorded for 'integrate' and 'volume' only");
+      if (mode == kVolume) return launch_walk_t<kVolume, 4, kOutTape>(cl, io, kernel, st);
+      if (cl->nfields == 1) return launch_walk_t<kSum, 1, kOutTape>(cl, io, kernel, st);
+      if (cl->nfields == 3) return launch_walk_t<kSum, 3, kOutTape>(cl, io, kernel, st);
+      if (cl->nfields == 4) return launch_walk_t<kSum, 4, kOutTape>(cl, io, kernel, st);
+      return launch_walk_t<kSum, 0, kOutTape>(cl, io, kernel, st);
+    default: return launch_walk_mode<kOutAdj>(cl, io, mode, kernel, st);
+  }
+}
+
+static int finish_walk(vt_cloud* cl, WalkIO& io, const DevStats& hs, float ms, cudaStream_t st,
+                       vt_stats* stats, WalkDiag* d_diag);
+
+// One walk launch (+ handed-over rays) on scratch already placed in `io`
+// (stats, hand-over queue, global stacks); turns a per-ray failure into the
+// reference's error message.  `d_diag`: device scratch for the diagnosis of
+// a failing ray (NULL: allocated on demand).  `timed`: CUDA events around
+// the launches for vt_stats.walk_ms.
+static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel,
+                       cudaStream_t st, vt_stats* stats, WalkDiag* d_diag, bool timed) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (timed) {
     VT_CUDA(cudaEventCreate(&e0));
     VT_CUDA(cudaEventCreate(&e1));
     VT_CUDA(cudaEventRecord(e0, st));
   }
-  int rc;
-  switch (out_kind) {
-    case kOutImage: rc = launch_walk_mode<kOutImage>(cl, io, mode, kernel, st); break;
-    case kOutCount: rc = launch_walk_mode<kOutCount>(cl, io, mode, kernel, st); break;
-    case kOutFill: rc = launch_walk_t<kSum, 1, kOutFill>(cl, io, kernel, st); break;
-    case kOutTape:
-      if (mode != kSum && mode != kVolume)
-        return set_error(VT_ERR_INVALID, "a tape is recorded for 'integrate' and 'volume' only");
-      if (mode == kVolume) rc = launch_walk_t<kVolume, 4, kOutTape>(cl, io, kernel, st);
-      else if (cl->nfields == 1) rc = launch_walk_t<kSum, 1, kOutTape>(cl, io, kernel, st);
-      else if (cl->nfields == 3) rc = launch_walk_t<kSum, 3, kOutTape>(cl, io, kernel, st);
-      else if (cl->nfields == 4) rc = launch_walk_t<kSum, 4, kOutTape>(cl, io, kernel, st);
-      else rc = launch_walk_t<kSum, 0, kOutTape>(cl, io, kernel, st);
-      break;
-    default: rc = launch_walk_mode<kOutAdj>(cl, io, mode, kernel, st); break;
-  }
+  const int rc = enqueue_walk(cl, io, out_kind, mode, kernel, st);
   if (rc) {
     if (timed) {
       cudaEventDestroy(e0);
@@ -507,6 +516,13 @@ static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int ker
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   }
+  return finish_walk(cl, io, hs, ms, st, stats, d_diag);
+}
+
+// Counters of a finished walk into `stats`; the reference's message when a
+// ray failed (the first failing ray is re-walked alone by k_diag).
+static int finish_walk(vt_cloud* cl, WalkIO& io, const DevStats& hs, float ms, cudaStream_t st,
+                       vt_stats* stats, WalkDiag* d_diag) {
   if (hs.rays > 0) cl->cross_per_ray = (double)hs.crossings / (double)hs.rays;
   if (stats) {
     stats->rays = hs.rays;
@@ -629,30 +645,50 @@ __global__ void k_ray_keys(const double* __restrict__ S, const double* __restric
   idx[i] = (int32_t)i;
 }
 
-// Fill io.order (workspace) with the coherent ray order.
-static int sort_rays(vt_cloud* cl, WalkIO& io, cudaStream_t st) {
-  const int64_t n = io.nrays;
-  io.order = nullptr;
-  if (n < 64 || n > (int64_t)0x7fffffff) return VT_OK;  // identity order
-  size_t cub_bytes = 0;
+// Scratch of the ray sort for n rays: keys and indices (twice) and CUB's
+// temporary storage; 0 when the rays keep their order (few or too many).
+static int sort_rays_bytes(int64_t n, size_t& total, size_t& cub_bytes) {
+  total = cub_bytes = 0;
+  if (n < 64 || n > (int64_t)0x7fffffff) return VT_OK;
   VT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (unsigned long long*)nullptr,
                                           (unsigned long long*)nullptr, (int32_t*)nullptr,
-                                          (int32_t*)nullptr, (int)n, 0, 63, st));
+                                          (int32_t*)nullptr, (int)n, 0, 63));
   const size_t kb = ((size_t)n * 8 + 255) & ~(size_t)255;
   const size_t ib = ((size_t)n * 4 + 255) & ~(size_t)255;
-  if (cl->ws_order.reserve(2 * kb + 2 * ib + cub_bytes)) return VT_ERR_NOMEM;
-  uint8_t* base = cl->ws_order.p;
+  total = 2 * kb + 2 * ib + cub_bytes;
+  return VT_OK;
+}
+
+// Enqueue the ray sort into `base` (sort_rays_bytes of scratch) and point
+// io.order at the result; no host synchronisation.
+static int sort_rays_into(const DevCloud& view, WalkIO& io, uint8_t* base, size_t total,
+                          size_t cub_bytes, cudaStream_t st) {
+  const int64_t n = io.nrays;
+  io.order = nullptr;
+  if (total == 0) return VT_OK;
+  const size_t kb = ((size_t)n * 8 + 255) & ~(size_t)255;
+  const size_t ib = ((size_t)n * 4 + 255) & ~(size_t)255;
   auto* k0 = reinterpret_cast<unsigned long long*>(base);
   auto* k1 = reinterpret_cast<unsigned long long*>(base + kb);
   auto* i0 = reinterpret_cast<int32_t*>(base + 2 * kb);
   auto* i1 = reinterpret_cast<int32_t*>(base + 2 * kb + ib);
   void* tmp = base + 2 * kb + 2 * ib;
   const int B = 256;
-  k_ray_keys<<<(unsigned)((n + B - 1) / B), B, 0, st>>>(io.starts, io.ends, n, cl->view, k0, i0);
+  k_ray_keys<<<(unsigned)((n + B - 1) / B), B, 0, st>>>(io.starts, io.ends, n, view, k0, i0);
   VT_CUDA(cudaGetLastError());
-  VT_CUDA(cub::DeviceRadixSort::SortPairs(tmp, cub_bytes, k0, k1, i0, i1, (int)n, 0, 63, st));
+  size_t cb = cub_bytes;
+  VT_CUDA(cub::DeviceRadixSort::SortPairs(tmp, cb, k0, k1, i0, i1, (int)n, 0, 63, st));
   io.order = i1;
   return VT_OK;
+}
+
+// Fill io.order (workspace) with the coherent ray order.
+static int sort_rays(vt_cloud* cl, WalkIO& io, cudaStream_t st) {
+  size_t total = 0, cub_bytes = 0;
+  int rc = sort_rays_bytes(io.nrays, total, cub_bytes);
+  if (rc) return rc;
+  if (total && (rc = cl->ws_order.reserve(total))) return rc;
+  return sort_rays_into(cl->view, io, cl->ws_order.p, total, cub_bytes, st);
 }
 
 // Walk launch with the handle's (grow-only) workspace as scratch.
@@ -677,6 +713,135 @@ int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaS
   io.slow_threads = slow_threads;
   return run_walk_on(cl, io, out_kind, mode, kernel, st, stats, nullptr, true);
 }
+
+}  // namespace vt
+
+// ------------------------------------------------------ CUDA graph of a walk
+// A forward projection of fixed device buffers captured once (counter
+// resets, ray sort, walk kernel, global-stack kernel) and replayed with one
+// cudaGraphLaunch.  The graph owns its scratch; it reads the rays and writes
+// the image through the pointers given at creation, so a caller refills the
+// same buffers between launches.
+struct vt_graph {
+  vt_cloud* cl = nullptr;
+  int device = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  vt::DevBuf<vt::DevStats> stats;
+  vt::DevBuf<unsigned long long> slow;
+  vt::DevBuf<int> stack_id;
+  vt::DevBuf<double> stack_s;
+  vt::DevBuf<uint8_t> order;
+  vt::WalkIO io{};
+  const double4* pts = nullptr;  // the cloud's buffers at capture time
+  const double* fields = nullptr;
+  ~vt_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
+
+extern "C" {
+
+int vt_graph_create(vt_cloud* cl, const double* d_starts, const double* d_ends, uint64_t nrays,
+                    int mode, int kernel, double* d_out, vt_graph** out) {
+  using namespace vt;
+  try {
+    if (!out) return set_error(VT_ERR_INVALID, "out must not be NULL");
+    *out = nullptr;
+    int rc = check_projectable(cl, mode);
+    if (rc) return rc;
+    if (nrays == 0 || !d_starts || !d_ends || !d_out)
+      return set_error(VT_ERR_INVALID, "a graph needs rays and device buffers");
+    std::lock_guard<std::mutex> lk(cl->mu);
+    VT_CUDA(cudaSetDevice(cl->device));
+    std::unique_ptr<vt_graph> g(new vt_graph());
+    g->cl = cl;
+    g->device = cl->device;
+    const int slow_threads = 1024;
+    if ((rc = g->stats.alloc(1)) || (rc = g->slow.alloc(nrays)) ||
+        (rc = g->stack_id.alloc((size_t)slow_threads * cl->stack_cap)) ||
+        (rc = g->stack_s.alloc((size_t)slow_threads * cl->stack_cap)))
+      return rc;
+    WalkIO& io = g->io;
+    io.starts = d_starts;
+    io.ends = d_ends;
+    io.nrays = (int64_t)nrays;
+    io.nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
+    io.out = d_out;
+    io.stats = g->stats.p;
+    io.slow_q = g->slow.p;
+    io.gstack_id = g->stack_id.p;
+    io.gstack_s = g->stack_s.p;
+    io.gstack_cap = cl->stack_cap;
+    io.slow_threads = slow_threads;
+    const int k = resolve_kernel(cl, kernel, nrays);
+    size_t total = 0, cub_bytes = 0;
+    if (k != VT_KERNEL_PLAIN_FP64 && !cl->periodic) {
+      if ((rc = sort_rays_bytes(io.nrays, total, cub_bytes))) return rc;
+      if (total && (rc = g->order.alloc(total))) return rc;
+    }
+    cudaStream_t cs = nullptr;
+    VT_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) {
+      cudaStreamDestroy(cs);
+      VT_CUDA(e);
+    }
+    rc = sort_rays_into(cl->view, io, g->order.p, total, cub_bytes, cs);
+    if (!rc) rc = enqueue_walk(cl, io, kOutImage, mode, k, cs);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(cs, &graph);
+    cudaStreamDestroy(cs);
+    if (rc || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (rc) return rc;
+      VT_CUDA(e);
+    }
+    g->graph = graph;
+    VT_CUDA(cudaGraphInstantiate(&g->exec, graph, 0));
+    g->pts = cl->view.pts;
+    g->fields = cl->view.fields;
+    *out = g.release();
+    return VT_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(VT_ERR_NOMEM, "host allocation failed");
+  }
+}
+
+int vt_graph_launch(vt_graph* g, void* stream) {
+  using namespace vt;
+  if (!g) return set_error(VT_ERR_INVALID, "null graph handle");
+  if (g->cl->view.pts != g->pts || g->cl->view.fields != g->fields)
+    return set_error(VT_ERR_RUNTIME,
+                     "the cloud's tree or fields were reallocated after the graph was created");
+  VT_CUDA(cudaSetDevice(g->device));
+  VT_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+  return VT_OK;
+}
+
+int vt_graph_finish(vt_graph* g, void* stream, vt_stats* stats) {
+  using namespace vt;
+  if (!g) return set_error(VT_ERR_INVALID, "null graph handle");
+  if (stats) memset(stats, 0, sizeof(*stats));
+  std::lock_guard<std::mutex> lk(g->cl->mu);
+  VT_CUDA(cudaSetDevice(g->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  DevStats hs;
+  VT_CUDA(cudaMemcpyAsync(&hs, g->io.stats, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  return finish_walk(g->cl, g->io, hs, 0.f, st, stats, nullptr);
+}
+
+void vt_graph_destroy(vt_graph* g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  delete g;
+}
+
+}  // extern "C"
+
+namespace vt {
 
 // Adjoint of 'integrate' from a tape: grad[pid, f] += gout[ray, f] * ds for
 // every entry.  The lanes of a warp holding the same cell add their terms

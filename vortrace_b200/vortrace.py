@@ -352,6 +352,23 @@ class ProjectionCloud:
         ids, r2 = self._cloud.knn(q, k)
         return np.where(ids >= 0, self.orig_ids[np.maximum(ids, 0)], -1), r2
 
+    def autotune(self, pos_start, pos_end, *, reduction="integrate",
+                 max_sample: int = 65536) -> dict:
+        """Time the walk kernels and shared-memory tree depths on a sample of
+        these rays (extension; not in the reference) and make the fastest
+        the ``'auto'`` kernel for batches at least as large as the sample.
+        Results do not change, only the speed.  Returns the choice."""
+        mode = self._validate_reduction(reduction)
+        S = self._prepare_array_for_backend(pos_start).reshape(-1, 3)
+        E = self._prepare_array_for_backend(pos_end).reshape(-1, 3)
+        if S.shape != E.shape:
+            raise ValueError("pos_start / pos_end must have identical shapes")
+        res = L.TuneResult()
+        L.check(self._cloud._lib.vt_cloud_autotune(self._cloud._h, L.dptr(S), L.dptr(E),
+                                                   S.shape[0], mode, int(max_sample),
+                                                   C.byref(res)))
+        return res.as_dict()
+
     def slice(self, extent, nres, depth: float) -> np.ndarray:
         """2D slice at constant depth: the nearest cell's field values at
         each pixel (vortrace/vortrace.py:347-383; src/slice.cpp:6-60).
