@@ -214,6 +214,17 @@ int vt_project_adjoint_device(vt_cloud *cloud, const double *d_starts, const dou
                               uint64_t nrays, int mode, const double *d_out,
                               const double *d_grad_out, double *d_grad_fields, void *stream);
 
+/* Saved trees: PointCloud::saveTreeToBytes / loadTreeFromBytes
+ * (src/pointcloud.cpp:214-281, used by vortrace/io.py:137-241).  The blob is
+ * this library's own (versioned; the permutation and node splits of the
+ * device tree, about 4 bytes per point plus 24 per internal node, and a hash
+ * of the filtered points); loading it onto a cloud with the same points
+ * restores the tree without building it.  vt_cloud_tree_save with buf ==
+ * NULL only stores the blob size in *size.  A blob that is not this
+ * library's (e.g. a nanoflann index) is refused with VT_ERR_INVALID. */
+int vt_cloud_tree_save(vt_cloud *cloud, void *buf, uint64_t cap, uint64_t *size);
+int vt_cloud_tree_load(vt_cloud *cloud, const void *buf, uint64_t size);
+
 /* CUDA graph of a forward projection (no reference counterpart): the
  * counter resets, the ray sort, the walk kernel and the global-stack kernel
  * for fixed device buffers (d_starts, d_ends: nrays x 3; d_out: nrays x nout)

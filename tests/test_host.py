@@ -68,3 +68,20 @@ def test_null_handles():
     assert lib.vt_segments_count(None) == 0
     lib.vt_cloud_destroy(None)
     lib.vt_segments_free(None)
+
+
+def test_grid_io_round_trip(tmp_path):
+    from vortrace_b200 import io as vio
+    data = np.arange(12.0).reshape(3, 4)
+    vio.save_grid(tmp_path / "g.npz", data, extent=[0, 1, 2, 3], metadata={"npix": 4, "f": "rho"})
+    d, meta = vio.load_grid(tmp_path / "g.npz")
+    np.testing.assert_array_equal(d, data)
+    assert meta["npix"] == 4 and meta["f"] == "rho"
+    np.testing.assert_array_equal(meta["extent"], [0, 1, 2, 3])
+    with pytest.raises(ValueError, match="Unknown format"):
+        vio.save_grid(tmp_path / "g.bin", data, fmt="bin")
+    try:
+        import h5py  # noqa: F401
+    except ImportError:
+        with pytest.raises(ImportError, match="h5py is required"):
+            vio.save_grid(tmp_path / "g.h5", data, fmt="hdf5")

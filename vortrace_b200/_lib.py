@@ -47,6 +47,7 @@ EXPORTS = (
     "vt_tape_create", "vt_tape_destroy", "vt_tape_size", "vt_project_device_tape",
     "vt_tape_adjoint_device", "vt_slice", "vt_brute_projection", "vt_cloud_autotune",
     "vt_graph_create", "vt_graph_launch", "vt_graph_finish", "vt_graph_destroy",
+    "vt_cloud_tree_save", "vt_cloud_tree_load",
 )
 
 
@@ -146,6 +147,8 @@ def load(path: str | None = None):
         L.vt_cloud_autotune.argtypes = [vp, dp, dp, u64, C.c_int, u64, C.POINTER(TuneResult)]
         L.vt_graph_create.argtypes = [vp, vp, vp, u64, C.c_int, C.c_int, vp, C.POINTER(vp)]
         L.vt_graph_launch.argtypes = [vp, vp]
+        L.vt_cloud_tree_save.argtypes = [vp, vp, u64, C.POINTER(u64)]
+        L.vt_cloud_tree_load.argtypes = [vp, vp, u64]
         L.vt_graph_finish.argtypes = [vp, vp, C.POINTER(Stats)]
         L.vt_graph_destroy.argtypes = [vp]
         L.vt_graph_destroy.restype = None
@@ -163,7 +166,8 @@ def load(path: str | None = None):
                      "vt_project_adjoint", "vt_project_adjoint_device", "vt_set_device",
                      "vt_tape_create", "vt_project_device_tape", "vt_tape_adjoint_device",
                      "vt_slice", "vt_brute_projection", "vt_cloud_autotune",
-                     "vt_graph_create", "vt_graph_launch", "vt_graph_finish"):
+                     "vt_graph_create", "vt_graph_launch", "vt_graph_finish",
+                     "vt_cloud_tree_save", "vt_cloud_tree_load"):
             getattr(L, name).restype = C.c_int
         L.vt_set_warning_callback(_warn_cb)
         _lib = L

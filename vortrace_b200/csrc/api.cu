@@ -286,6 +286,38 @@ int vt_cloud_build_tree(vt_cloud* cl) {
   VT_GUARD_END
 }
 
+int vt_cloud_tree_save(vt_cloud* cl, void* buf, uint64_t cap, uint64_t* size) {
+  VT_GUARD_BEGIN
+  if (!cl || !size) return set_error(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  if (!cl->tree_built)
+    return set_error(VT_ERR_RUNTIME, "There is currently no valid tree for this point cloud");
+  *size = vt::tree_blob_size(cl);
+  if (!buf) return VT_OK;
+  if (cap < *size) return set_error(VT_ERR_INVALID, "buffer too small for the tree blob");
+  VT_CUDA(cudaSetDevice(cl->device));
+  return vt::save_tree_blob(cl, buf);
+  VT_GUARD_END
+}
+
+int vt_cloud_tree_load(vt_cloud* cl, const void* buf, uint64_t size) {
+  VT_GUARD_BEGIN
+  if (!cl || !buf) return set_error(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  if (cl->npart == 0)
+    return set_error(VT_ERR_RUNTIME, "There are no points in the cloud; cannot build tree");
+  VT_CUDA(cudaSetDevice(cl->device));
+  auto t0 = std::chrono::high_resolution_clock::now();
+  cl->tree_built = false;
+  int rc = vt::load_tree_blob(cl, buf, size);
+  if (rc) return rc;
+  auto t1 = std::chrono::high_resolution_clock::now();
+  cl->build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  cl->tree_built = true;
+  return VT_OK;
+  VT_GUARD_END
+}
+
 int vt_cloud_set_param(vt_cloud* cl, int param, int64_t value) {
   if (!cl) return set_error(VT_ERR_INVALID, "null cloud handle");
   std::lock_guard<std::mutex> lk(cl->mu);

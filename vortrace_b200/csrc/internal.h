@@ -150,6 +150,10 @@ struct vt_tape {
 
 namespace vt {
 int build_tree_device(vt_cloud* cl);
+// saved trees (tree_build.cu)
+uint64_t tree_blob_size(const vt_cloud* cl);
+int save_tree_blob(vt_cloud* cl, void* buf);
+int load_tree_blob(vt_cloud* cl, const void* buf, uint64_t size);
 int upload_fields(vt_cloud* cl, const double* src, bool src_device, cudaStream_t st);
 // tree built, mode valid, volume needs valid RGBA (src/reduction.cpp:59-66)
 int check_projectable(const vt_cloud* cl, int mode);

@@ -27,6 +27,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "common.cuh"
@@ -312,9 +313,97 @@ int upload_fields(vt_cloud* cl, const double* src, bool src_device, cudaStream_t
 }
 
 // Build the device tree of `cl` from its host points/fields.
-int build_tree_device(vt_cloud* cl) {
+// Tree-order point copies, node boxes, tree-order fields and the device
+// view, from the permutation (tree index -> internal id), the node splits
+// and the tree-ordered coordinates; shared by the build and the load of a
+// saved tree.
+static int finish_tree(vt_cloud* cl, int depth, const double lo[3], const double hi[3],
+                       const double org[3], DevBuf<int32_t>& pa, DevBuf<double2>& nodes,
+                       DevBuf<float2>& nodes32, const double* x, const double* y,
+                       const double* z) {
   const int64_t n = (int64_t)cl->npart;
   const int nf = (int)cl->nfields;
+  cudaStream_t st = cl->stream;
+  const int B = 256;
+  const int64_t nleaves = 1LL << depth;
+  int rc;
+#define VT_TRY(x)                      \
+  do {                                 \
+    if ((rc = (x)) != VT_OK) return rc; \
+  } while (0)
+  // tree-order copies
+  DevBuf<double4> pts;
+  DevBuf<float4> pts32;
+  DevBuf<double> fields;
+  VT_TRY(pts.alloc(n));
+  VT_TRY(pts32.alloc(n));
+  VT_TRY(fields.alloc((int64_t)n * nf));
+  k_finalize<<<nblk(n, B), B, 0, st>>>(x, y, z, n, org[0], org[1], org[2], pts.p, pts32.p);
+  DevBuf<float4> blo, bhi;
+  VT_TRY(blo.alloc(2 * nleaves - 1));
+  VT_TRY(bhi.alloc(2 * nleaves - 1));
+  k_leaf_boxes<<<nblk(nleaves, B), B, 0, st>>>(pts32.p, n, depth, nleaves, blo.p, bhi.p);
+  for (int l = depth - 1; l >= 0; --l)
+    k_level_boxes<<<nblk(1LL << l, B), B, 0, st>>>(l, blo.p, bhi.p);
+  {
+    // fields: upload in internal order into the (now free) aos buffer, gather
+    DevBuf<double> fin;
+    VT_TRY(fin.alloc((int64_t)n * nf));
+    VT_CUDA(cudaMemcpyAsync(fin.p, cl->fields.data(), (size_t)n * nf * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+    k_fields_tree<<<nblk((int64_t)n * nf, B), B, 0, st>>>(fin.p, pa.p, n, nf, fields.p);
+    VT_CUDA(cudaGetLastError());
+    VT_CUDA(cudaStreamSynchronize(st));
+  }
+  // largest |p - origin| component, for the FP32 error bounds
+  double mext = 0.0;
+  for (int j = 0; j < 3; ++j) mext = fmax(mext, fmax(fabs(hi[j] - org[j]), fabs(lo[j] - org[j])));
+
+  cl->perm_d = std::move(pa);
+  cl->pts_d = std::move(pts);
+  cl->pts32_d = std::move(pts32);
+  cl->nodes_d = std::move(nodes);
+  cl->nodes32_d = std::move(nodes32);
+  cl->fields_d = std::move(fields);
+  cl->boxlo_d = std::move(blo);
+  cl->boxhi_d = std::move(bhi);
+  DevCloud& v = cl->view;
+  v.pts = cl->pts_d.p;
+  v.pts32 = cl->pts32_d.p;
+  v.nodes = cl->nodes_d.p;
+  v.nodes32 = cl->nodes32_d.p;
+  v.perm = cl->perm_d.p;
+  v.fields = cl->fields_d.p;
+  v.boxlo = cl->boxlo_d.p;
+  v.boxhi = cl->boxhi_d.p;
+  v.n = n;
+  v.nleaves = nleaves;
+  v.nf = nf;
+  v.depth = depth;
+  for (int j = 0; j < 3; ++j) {
+    v.bblo[j] = lo[j];
+    v.bbhi[j] = hi[j];
+    v.origin[j] = org[j];
+    // outward-rounded FP32 root box (all pts32 lie inside it)
+    v.bblo32[j] = std::nextafter((float)(lo[j] - org[j]), -INFINITY);
+    v.bbhi32[j] = std::nextafter((float)(hi[j] - org[j]), INFINITY);
+    v.bblo32[j] = std::nextafter(v.bblo32[j], -INFINITY);
+    v.bbhi32[j] = std::nextafter(v.bbhi32[j], INFINITY);
+  }
+  // |fl32(p - o) - (p - o)| <= 2^-24 |p - o| (plus the FP64 subtraction)
+  v.coord_err = (float)(mext * 6.0e-8 + 1e-300);
+  v.periodic = cl->periodic ? 1 : 0;
+  for (int j = 0; j < 3; ++j) {
+    v.sub_lo[j] = cl->subbox[2 * j];
+    v.sub_hi[j] = cl->subbox[2 * j + 1];
+    v.box[j] = cl->subbox[2 * j + 1] - cl->subbox[2 * j];
+  }
+  return VT_OK;
+#undef VT_TRY
+}
+
+int build_tree_device(vt_cloud* cl) {
+  const int64_t n = (int64_t)cl->npart;
   cudaStream_t st = cl->stream;
   const int B = 256;
   int depth = 0;
@@ -419,76 +508,124 @@ int build_tree_device(vt_cloud* cl) {
   }
   VT_CUDA(cudaGetLastError());
 
-  // 4. tree-order copies
-  DevBuf<double4> pts;
-  DevBuf<float4> pts32;
-  DevBuf<double> fields;
-  VT_TRY(pts.alloc(n));
-  VT_TRY(pts32.alloc(n));
-  VT_TRY(fields.alloc((int64_t)n * nf));
-  k_finalize<<<nblk(n, B), B, 0, st>>>(ax.p, ay.p, az.p, n, org[0], org[1], org[2], pts.p,
-                                       pts32.p);
-  DevBuf<float4> blo, bhi;
-  VT_TRY(blo.alloc(2 * nleaves - 1));
-  VT_TRY(bhi.alloc(2 * nleaves - 1));
-  k_leaf_boxes<<<nblk(nleaves, B), B, 0, st>>>(pts32.p, n, depth, nleaves, blo.p, bhi.p);
-  for (int l = depth - 1; l >= 0; --l)
-    k_level_boxes<<<nblk(1LL << l, B), B, 0, st>>>(l, blo.p, bhi.p);
-  {
-    // fields: upload in internal order into the (now free) aos buffer, gather
-    DevBuf<double> fin;
-    VT_TRY(fin.alloc((int64_t)n * nf));
-    VT_CUDA(cudaMemcpyAsync(fin.p, cl->fields.data(), (size_t)n * nf * sizeof(double),
-                            cudaMemcpyHostToDevice, st));
-    k_fields_tree<<<nblk((int64_t)n * nf, B), B, 0, st>>>(fin.p, pa.p, n, nf, fields.p);
-    VT_CUDA(cudaGetLastError());
-    VT_CUDA(cudaStreamSynchronize(st));
-  }
-  // largest |p - origin| component, for the FP32 error bounds
-  double mext = 0.0;
-  for (int j = 0; j < 3; ++j) mext = fmax(mext, fmax(fabs(hi[j] - org[j]), fabs(lo[j] - org[j])));
-
-  cl->perm_d = std::move(pa);
-  cl->pts_d = std::move(pts);
-  cl->pts32_d = std::move(pts32);
-  cl->nodes_d = std::move(nodes);
-  cl->nodes32_d = std::move(nodes32);
-  cl->fields_d = std::move(fields);
-  cl->boxlo_d = std::move(blo);
-  cl->boxhi_d = std::move(bhi);
-  DevCloud& v = cl->view;
-  v.pts = cl->pts_d.p;
-  v.pts32 = cl->pts32_d.p;
-  v.nodes = cl->nodes_d.p;
-  v.nodes32 = cl->nodes32_d.p;
-  v.perm = cl->perm_d.p;
-  v.fields = cl->fields_d.p;
-  v.boxlo = cl->boxlo_d.p;
-  v.boxhi = cl->boxhi_d.p;
-  v.n = n;
-  v.nleaves = nleaves;
-  v.nf = nf;
-  v.depth = depth;
-  for (int j = 0; j < 3; ++j) {
-    v.bblo[j] = lo[j];
-    v.bbhi[j] = hi[j];
-    v.origin[j] = org[j];
-    // outward-rounded FP32 root box (all pts32 lie inside it)
-    v.bblo32[j] = std::nextafter((float)(lo[j] - org[j]), -INFINITY);
-    v.bbhi32[j] = std::nextafter((float)(hi[j] - org[j]), INFINITY);
-    v.bblo32[j] = std::nextafter(v.bblo32[j], -INFINITY);
-    v.bbhi32[j] = std::nextafter(v.bbhi32[j], INFINITY);
-  }
-  // |fl32(p - o) - (p - o)| <= 2^-24 |p - o| (plus the FP64 subtraction)
-  v.coord_err = (float)(mext * 6.0e-8 + 1e-300);
-  v.periodic = cl->periodic ? 1 : 0;
-  for (int j = 0; j < 3; ++j) {
-    v.sub_lo[j] = cl->subbox[2 * j];
-    v.sub_hi[j] = cl->subbox[2 * j + 1];
-    v.box[j] = cl->subbox[2 * j + 1] - cl->subbox[2 * j];
-  }
-  return VT_OK;
+  return finish_tree(cl, depth, lo, hi, org, pa, nodes, nodes32, ax.p, ay.p, az.p);
 #undef VT_TRY
+}
+
+// ------------------------------------------------------- saved trees
+// Blob: TreeBlobHeader, then perm (int32 x n), nodes (double2 x L-1) and
+// nodes32 (float2 x L-1).  The boxes, the tree-order copies and the fields
+// are rebuilt from the cloud's own points, which must be the ones the tree
+// was built on: the header keeps a hash of them.
+struct TreeBlobHeader {
+  char magic[8];
+  uint32_t version;
+  uint32_t depth;
+  uint64_t n;
+  uint64_t leaf_size;
+  double lo[3], hi[3], org[3];
+  uint64_t points_hash;
+};
+static const char kTreeMagic[8] = {'V', 'T', 'B', '2', 'T', 'R', 'E', 'E'};
+
+// 64-bit hash of the filtered points (word-wise multiply-xor).
+static uint64_t points_hash(const std::vector<double>& p) {
+  uint64_t h = 1469598103934665603ULL;
+  for (double v : p) {
+    uint64_t w;
+    memcpy(&w, &v, 8);
+    h = (h ^ w) * 1099511628211ULL;
+    h ^= h >> 29;
+  }
+  return h;
+}
+
+__global__ void k_gather_aos(const double* __restrict__ aos, const int32_t* __restrict__ perm,
+                             int64_t n, double* x, double* y, double* z) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t p = perm[i];
+  x[i] = aos[3 * p];
+  y[i] = aos[3 * p + 1];
+  z[i] = aos[3 * p + 2];
+}
+
+uint64_t tree_blob_size(const vt_cloud* cl) {
+  const int64_t ni = cl->view.nleaves - 1;
+  return sizeof(TreeBlobHeader) + (uint64_t)cl->npart * 4 + (uint64_t)ni * (16 + 8);
+}
+
+int save_tree_blob(vt_cloud* cl, void* buf) {
+  TreeBlobHeader hd;
+  memcpy(hd.magic, kTreeMagic, 8);
+  hd.version = 1;
+  hd.depth = (uint32_t)cl->view.depth;
+  hd.n = cl->npart;
+  hd.leaf_size = (uint64_t)cl->leaf_size;
+  for (int j = 0; j < 3; ++j) {
+    hd.lo[j] = cl->view.bblo[j];
+    hd.hi[j] = cl->view.bbhi[j];
+    hd.org[j] = cl->view.origin[j];
+  }
+  hd.points_hash = points_hash(cl->pts);
+  uint8_t* out = static_cast<uint8_t*>(buf);
+  memcpy(out, &hd, sizeof(hd));
+  out += sizeof(hd);
+  const int64_t ni = cl->view.nleaves - 1;
+  cudaStream_t st = cl->stream;
+  VT_CUDA(cudaMemcpyAsync(out, cl->perm_d.p, cl->npart * 4, cudaMemcpyDeviceToHost, st));
+  out += cl->npart * 4;
+  if (ni > 0) {
+    VT_CUDA(cudaMemcpyAsync(out, cl->nodes_d.p, ni * 16, cudaMemcpyDeviceToHost, st));
+    out += ni * 16;
+    VT_CUDA(cudaMemcpyAsync(out, cl->nodes32_d.p, ni * 8, cudaMemcpyDeviceToHost, st));
+  }
+  VT_CUDA(cudaStreamSynchronize(st));
+  return VT_OK;
+}
+
+int load_tree_blob(vt_cloud* cl, const void* buf, uint64_t size) {
+  TreeBlobHeader hd;
+  if (size < sizeof(hd)) return set_error(VT_ERR_INVALID, "tree blob too short");
+  memcpy(&hd, buf, sizeof(hd));
+  if (memcmp(hd.magic, kTreeMagic, 8) != 0)
+    return set_error(VT_ERR_INVALID, "not a libvortrace_b200 tree blob");
+  if (hd.version != 1) return set_error(VT_ERR_INVALID, "unsupported tree blob version");
+  const int64_t n = (int64_t)cl->npart;
+  if (hd.n != (uint64_t)n || hd.depth > (uint32_t)kMaxDepth ||
+      ((n + (1LL << hd.depth) - 1) >> hd.depth) > (int64_t)hd.leaf_size || hd.leaf_size < 1)
+    return set_error(VT_ERR_INVALID, "tree blob does not fit this point cloud");
+  const int depth = (int)hd.depth;
+  const int64_t ni = (1LL << depth) - 1;
+  if (size != sizeof(hd) + (uint64_t)n * 4 + (uint64_t)ni * 24)
+    return set_error(VT_ERR_INVALID, "tree blob has the wrong size");
+  if (hd.points_hash != points_hash(cl->pts))
+    return set_error(VT_ERR_INVALID, "tree blob was built on other points");
+  const uint8_t* in = static_cast<const uint8_t*>(buf) + sizeof(hd);
+  cudaStream_t st = cl->stream;
+  const int B = 256;
+  int rc;
+  DevBuf<int32_t> pa;
+  DevBuf<double2> nodes;
+  DevBuf<float2> nodes32;
+  DevBuf<double> aos, x, y, z;
+  if ((rc = pa.alloc(n)) || (rc = nodes.alloc(ni > 0 ? ni : 1)) ||
+      (rc = nodes32.alloc(ni > 0 ? ni : 1)) || (rc = aos.alloc(3 * n)) || (rc = x.alloc(n)) ||
+      (rc = y.alloc(n)) || (rc = z.alloc(n)))
+    return rc;
+  VT_CUDA(cudaMemcpyAsync(pa.p, in, n * 4, cudaMemcpyHostToDevice, st));
+  in += n * 4;
+  if (ni > 0) {
+    VT_CUDA(cudaMemcpyAsync(nodes.p, in, ni * 16, cudaMemcpyHostToDevice, st));
+    in += ni * 16;
+    VT_CUDA(cudaMemcpyAsync(nodes32.p, in, ni * 8, cudaMemcpyHostToDevice, st));
+  }
+  VT_CUDA(cudaMemcpyAsync(aos.p, cl->pts.data(), 3 * n * sizeof(double), cudaMemcpyHostToDevice,
+                          st));
+  k_gather_aos<<<nblk(n, B), B, 0, st>>>(aos.p, pa.p, n, x.p, y.p, z.p);
+  VT_CUDA(cudaGetLastError());
+  cl->leaf_size = (int)hd.leaf_size;
+  return finish_tree(cl, depth, hd.lo, hd.hi, hd.org, pa, nodes, nodes32, x.p, y.p, z.p);
 }
 
 }  // namespace vt

@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes as C
 import logging
+import warnings
 
 import numpy as np
 
@@ -95,6 +96,26 @@ class _Cloud:
 
     def set_param(self, param, value):
         L.check(self._lib.vt_cloud_set_param(self._h, param, int(value)))
+
+    # tree persistence (src/bindings.cpp:119-133)
+    def saveTreeToBytes(self) -> bytes:
+        size = C.c_uint64()
+        L.check(self._lib.vt_cloud_tree_save(self._h, None, 0, C.byref(size)))
+        buf = C.create_string_buffer(size.value)
+        L.check(self._lib.vt_cloud_tree_save(self._h, buf, size.value, C.byref(size)))
+        return buf.raw[:size.value]
+
+    def loadTreeFromBytes(self, data: bytes):
+        data = bytes(data)
+        L.check(self._lib.vt_cloud_tree_load(self._h, data, len(data)))
+
+    def saveTree(self, filename):
+        with open(filename, "wb") as f:
+            f.write(self.saveTreeToBytes())
+
+    def loadTree(self, filename):
+        with open(filename, "rb") as f:
+            self.loadTreeFromBytes(f.read())
 
     def queryTree(self, q, k=None):
         """PointCloud.queryTree (src/bindings.cpp:155-174): nearest id, or
@@ -368,6 +389,40 @@ class ProjectionCloud:
                                                    S.shape[0], mode, int(max_sample),
                                                    C.byref(res)))
         return res.as_dict()
+
+    # ------------------------------------------------ tree serialization
+    TREE_MAGIC = b"VTB2TREE"
+
+    def save_tree_bytes(self) -> bytes | None:
+        """The device tree as bytes (this library's blob), or None if not
+        built (vortrace/vortrace.py:389-393)."""
+        if self._cloud.get_tree_built():
+            return self._cloud.saveTreeToBytes()
+        return None
+
+    def load_tree_bytes(self, data: bytes) -> None:
+        """Restore the tree from :meth:`save_tree_bytes` output.  A blob of
+        another library (e.g. the reference's nanoflann index) cannot be used
+        by the device walk: the tree is then built on the device instead."""
+        data = bytes(data)
+        if data[:8] != self.TREE_MAGIC:
+            warnings.warn("tree blob is not a vortrace_b200 device tree (e.g. a nanoflann "
+                          "index); rebuilding the tree on the device", UserWarning,
+                          stacklevel=2)
+            self._cloud.buildTree()
+            return
+        self._cloud.loadTreeFromBytes(data)
+
+    def save(self, filename, *, fmt: str = "npz", save_tree: bool = True) -> None:
+        """Save this cloud (see :func:`vortrace_b200.io.save_cloud`)."""
+        from .io import save_cloud
+        save_cloud(filename, self, fmt=fmt, save_tree=save_tree)
+
+    @classmethod
+    def load(cls, filename) -> "ProjectionCloud":
+        """Load a cloud (see :func:`vortrace_b200.io.load_cloud`)."""
+        from .io import load_cloud
+        return load_cloud(filename)
 
     def slice(self, extent, nres, depth: float) -> np.ndarray:
         """2D slice at constant depth: the nearest cell's field values at
