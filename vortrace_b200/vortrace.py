@@ -4,11 +4,16 @@ reference's ``vortrace.ProjectionCloud`` (vortrace/vortrace.py:24-419).
 Same constructor, methods, argument handling, output shapes and exceptions
 as the reference; the work runs in libvortrace_b200.so (C ABI, ctypes) on a
 B200.  Extras that do not change the reference's calls:
-  * ``kernel`` attribute: ``'auto'`` (batched guarded-FP32 kernel),
-    ``'plain'`` (one ray per thread, FP64), ``'batched'``, ``'batched_fp64'``;
+  * ``kernel`` attribute: ``'auto'`` (the batched guarded-FP32 kernel, one ray
+    per thread; one ray per warp below 65,536 rays; or the autotuner's
+    choice), ``'thread_fp32'``, ``'batched_fp64'``, ``'batched'`` (one ray per
+    warp), ``'plain'`` (one ray per thread in the caller's order, FP64);
   * ``last_stats``: counters of the last projection (rays, crossings,
     queries, FP64 re-resolves, handed-over rays, walk time);
-  * :meth:`batch_projection`: many grids and arbitrary rays in one launch.
+  * :meth:`batch_projection`: many grids and arbitrary rays in one launch;
+  * :meth:`autotune`: kernel and shared-memory tree depth from timings;
+  * :meth:`slice`, :class:`Slice`, :class:`BruteProjection`, :meth:`save` /
+    :meth:`load` as in the reference (nearest-cell sampling, persistence).
 """
 from __future__ import annotations
 
