@@ -10,8 +10,9 @@ reference's timing of Projection::makeProjection excludes buildTree).
 Prints one JSON line (rank 0).
 
 Metric: cell crossings per second (Mcrossings/s) of the batched kernel
-(VT_KERNEL_AUTO: persistent, one ray per thread, rays in a coherent sorted
-order, bounded guarded-FP32 k-NN with FP64 re-checks), forward; the same
+(VT_KERNEL_AUTO after vt_cloud_autotune on the workload's rays: persistent,
+one ray per thread in a coherent sorted order with the bounded guarded-FP32
+or FP64 k-NN, or one ray per warp for small batches), forward; the same
 line reports forward+adjoint, the bounded-FP64 variant of the batched
 kernel and the plain FP64 one-ray-per-thread kernel.  Multi-GPU (torchrun): every rank projects its own
 view of the cloud (the grid rotated about the cloud centre by 2*pi*rank/N):
@@ -316,6 +317,12 @@ def run_ours(args):
         return float(t.item())
 
     K, W = args.steps, args.warmup
+    # --- autotune (outside the timed region): the AUTO kernel and the
+    # shared-memory tree depth from timings on a sample of this workload's rays
+    tune = pc.autotune(S, E, reduction={L.REDUCE_VOLUME: "volume"}.get(mode, "integrate"))
+    auto_kernel = tune["kernel"] if n >= tune["sample_rays"] else (
+        "batched" if n < 65536 else "thread_fp32")
+
     # --- forward, batched kernel (the headline)
     for _ in range(W):
         fwd(L.KERNEL_AUTO)
@@ -421,12 +428,15 @@ def run_ours(args):
     roof = None
     if bx and launch_ms:
         achieved = crossings * bx / (launch_ms / 1e3) / 1e9
-        dpc = DRAM_BYTES_PER_CROSSING.get(args.config)
+        # (measured for the guarded-FP32 kernel)
+        dpc = DRAM_BYTES_PER_CROSSING.get(args.config) if auto_kernel == "thread_fp32" else None
         traffic = round(dpc * crossings) if dpc else None
         roof = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "peak_source": peak_src, "bytes_per_crossing": bx,
-                "kernel": "k_batched (guarded-FP32 k-NN, coherent ray order)"}
+                "kernel": {"thread_fp32": "k_batched (guarded-FP32 k-NN, coherent ray order)",
+                           "batched_fp64": "k_batched (bounded FP64 k-NN, coherent ray order)",
+                           "batched": "k_warp (one ray per warp)"}.get(auto_kernel, auto_kernel)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -455,7 +465,8 @@ def run_ours(args):
                                 "B/crossing) + scatter" if taped and tape_entries > 0
                                 else "re-walk"),
             "fwd_bwd_rewalk_mcrossings_per_s": round(rw_value, 4),
-            "kernel": "batched (VT_KERNEL_AUTO = VT_KERNEL_THREAD_FP32)",
+            "kernel": f"VT_KERNEL_AUTO = {auto_kernel}",
+            "autotune": tune,
             "bounded_fp64_mcrossings_per_s": round(f64_value, 4),
             "plain_fp64_mcrossings_per_s": round(pl_value, 4),
             "speedup_vs_plain_fp64": round(value / pl_value, 3),

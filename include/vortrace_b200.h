@@ -243,7 +243,7 @@ void vt_graph_destroy(vt_graph *graph);
 /* Autotuner (no reference counterpart).  Times the walk kernels (one ray
  * per thread with the guarded-FP32 or the FP64 search, one ray per warp) and
  * the number of tree levels staged in shared memory (0-9) on a sample of
- * the given rays (host arrays, nrays x 3) -- up to max_sample (0: 65,536)
+ * the given rays (host arrays, nrays x 3) -- up to max_sample (0: 262,144)
  * rays in four contiguous
  * blocks, each configuration run twice, the second run timed -- and makes
  * the fastest the cloud's VT_KERNEL_AUTO choice for batches at least as

@@ -707,7 +707,10 @@ int vt_cloud_autotune(vt_cloud* cl, const double* starts, const double* ends, ui
   std::lock_guard<std::mutex> lk(cl->mu);
   VT_CUDA(cudaSetDevice(cl->device));
   if (nrays == 0) return set_error(VT_ERR_INVALID, "autotune needs at least one ray");
-  if (max_sample == 0) max_sample = 65536;
+  // the sample must fill the device several times over (148 SMs x 5 blocks
+  // x 128 threads ~ 95K rays resident), or it favours configurations that
+  // cope with low occupancy
+  if (max_sample == 0) max_sample = 262144;
   const uint64_t m = nrays < max_sample ? nrays : max_sample;
   if (!starts || !ends) return set_error(VT_ERR_INVALID, "starts/ends must not be NULL");
   cudaStream_t st = cl->stream;

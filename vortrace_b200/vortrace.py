@@ -379,7 +379,7 @@ class ProjectionCloud:
         return np.where(ids >= 0, self.orig_ids[np.maximum(ids, 0)], -1), r2
 
     def autotune(self, pos_start, pos_end, *, reduction="integrate",
-                 max_sample: int = 65536) -> dict:
+                 max_sample: int = 262144) -> dict:
         """Time the walk kernels and shared-memory tree depths on a sample of
         these rays (extension; not in the reference) and make the fastest
         the ``'auto'`` kernel for batches at least as large as the sample.
