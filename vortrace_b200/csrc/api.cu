@@ -843,9 +843,7 @@ int vt_project_device_tape(vt_cloud* cl, vt_tape* tape, const double* d_starts,
   io.tape = tape->buf.p;
   io.tape_count = tape->count.p;
   io.tape_cap = tape->cap;
-  // the warp-per-ray kernel keeps no tape: AUTO and BATCHED run one ray per thread
-  int k = resolve_kernel(cl, kernel, nrays);
-  if (k == VT_KERNEL_BATCHED) k = VT_KERNEL_THREAD_FP32;
+  const int k = resolve_kernel(cl, kernel, nrays);
   if ((rc = vt::run_walk(cl, io, vt::kOutTape, mode, k, st, stats))) return rc;
   unsigned long long used = 0;
   VT_CUDA(cudaMemcpyAsync(&used, tape->count.p, sizeof(used), cudaMemcpyDeviceToHost, st));

@@ -400,11 +400,9 @@ static int launch_walk_t(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) 
       k_plain<MODE, NF, OUT, true><<<(unsigned)((io.nrays + B - 1) / B), B, 0, st>>>(c, io);
     } else if (kernel == VT_KERNEL_PLAIN_FP64) {
       k_plain<MODE, NF, OUT, false><<<(unsigned)((io.nrays + B - 1) / B), B, 0, st>>>(c, io);
-    } else if (OUT != kOutTape && kernel == VT_KERNEL_BATCHED && cl->nfields <= 32) {
-      if constexpr (OUT != kOutTape) {
-        int rc = launch_warp<MODE, OUT>(cl, io, st);
-        if (rc) return rc;
-      }
+    } else if (kernel == VT_KERNEL_BATCHED && cl->nfields <= 32) {
+      int rc = launch_warp<MODE, OUT>(cl, io, st);
+      if (rc) return rc;
     } else {
       int rc = launch_batched<MODE, NF, OUT>(cl, io, kernel, st);
       if (rc) return rc;

@@ -703,12 +703,25 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
     WarpAdj<MODE> adj;
     unsigned fill_n = 0;
     int64_t fill_off = 0;
-    if (OUT == kOutImage || OUT == kOutCount) red.init();
+    if (OUT == kOutImage || OUT == kOutCount || OUT == kOutTape) red.init();
     else if (OUT == kOutFill) fill_off = io.offsets[ray];
     else adj.init(io, lane, ray, 0u);
     auto emit = [&](int cell, double a, double b) {
       if (OUT == kOutImage || OUT == kOutCount) red.seg(c, lane, cell, a, b);
-      else if (OUT == kOutFill) {
+      else if (OUT == kOutTape) {
+        // the reducer, then lane 0 records the segment (for 'volume' with the
+        // transmittance in front of it and the colour composited up to it)
+        const double T0 = red.T;
+        red.seg(c, lane, cell, a, b);
+        if (MODE == kVolume) {
+          const double p0 = __shfl_sync(kFull, red.acc, 0);
+          const double p1 = __shfl_sync(kFull, red.acc, 1);
+          const double p2 = __shfl_sync(kFull, red.acc, 2);
+          if (lane == 0) tape_append(io, TapeEntryV{cell, (int)ray, dsub(b, a), T0, {p0, p1, p2}});
+        } else if (lane == 0) {
+          tape_append(io, TapeEntry{c.perm[cell], (int)ray, dsub(b, a)});
+        }
+      } else if (OUT == kOutFill) {
         if (lane == 0) {
           io.seg_cell[fill_off + fill_n] = c.perm[cell];
           io.seg_enter[fill_off + fill_n] = a;
@@ -718,7 +731,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
       } else adj.seg(c, io, lane, cell, a, b);
     };
     auto nseg_now = [&]() -> unsigned {
-      return (OUT == kOutImage || OUT == kOutCount) ? red.nseg : (OUT == kOutFill ? fill_n : adj.nseg);
+      return (OUT == kOutImage || OUT == kOutCount || OUT == kOutTape)
+                 ? red.nseg
+                 : (OUT == kOutFill ? fill_n : adj.nseg);
     };
 
     // ---- end cells: leaf on the split-plane path, then a bounded search
@@ -954,7 +969,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
       if (rc == 0) emit(open_cell, entry_s, cur_s);
     }
     if (rc == 0) {
-      if (OUT == kOutImage || OUT == kOutCount) {
+      if (OUT == kOutImage || OUT == kOutCount || OUT == kOutTape) {
         if (lane < io.nout) io.out[ray * io.nout + lane] = red.acc;
         if (OUT == kOutCount && lane == 0) io.counts[ray] = red.nseg;
       }
