@@ -33,10 +33,13 @@ constexpr int kBatchStack = 32;
 #ifndef VT_BATCHED_MINB
 #define VT_BATCHED_MINB 5
 #endif
-// FP32 search stack entries: 0 = (node, bound, per-axis offsets), 1 = (node,
-// bound) with the offsets restarted from zero below a popped node
-#ifndef VT_STACK_NM
-#define VT_STACK_NM 0
+// points per batch of distances in a leaf scan of the FP32 / FP64 searches
+// (0: one at a time)
+#ifndef VT_LEAF_BATCH
+#define VT_LEAF_BATCH 4
+#endif
+#ifndef VT_LEAF_BATCH64
+#define VT_LEAF_BATCH64 4
 #endif
 
 // ---- node fetch (shared memory for the top levels) ----------------------
@@ -115,6 +118,25 @@ __device__ __forceinline__ void knn64_fetch(const DevCloud& c, const F& fetch, d
     {
       int64_t a, b;
       leaf_range(c, node - ninternal, a, b);
+#if VT_LEAF_BATCH64
+      // FP64 distances of up to VT_LEAF_BATCH64 points first (their loads in
+      // flight together), then the tests in point order
+      for (int64_t p0 = a; p0 < b; p0 += VT_LEAF_BATCH64) {
+        double db[VT_LEAF_BATCH64];
+#pragma unroll
+        for (int j = 0; j < VT_LEAF_BATCH64; ++j) {
+          db[j] = __longlong_as_double(0x7ff0000000000000ULL);
+          if (p0 + j < b) db[j] = metric(qx, qy, qz, ldg_pt(&c.pts[p0 + j]));
+        }
+#pragma unroll
+        for (int j = 0; j < VT_LEAF_BATCH64; ++j) {
+          if (db[j] < thr) {
+            res.insert(db[j], (int)(p0 + j));
+            thr = fmin(bound, res.worst());
+          }
+        }
+      }
+#else
       for (int64_t p = a; p < b; ++p) {
         const double d = metric(qx, qy, qz, ldg_pt(&c.pts[p]));
         if (d < thr) {
@@ -122,6 +144,7 @@ __device__ __forceinline__ void knn64_fetch(const DevCloud& c, const F& fetch, d
           thr = fmin(bound, res.worst());
         }
       }
+#endif
     }
     bool found = false;
     while (sp > 0) {
@@ -165,14 +188,9 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
   const int64_t ninternal = c.nleaves - 1;
   int node = 0;
   int sp = 0;
-#if VT_STACK_NM
-  int2 s_e[kMaxDepth + 2];  // (node, bound)
-  float base = 0.f;         // bound of the subtree being searched
-#else
   int s_node[kMaxDepth + 2];
   float s_off[kMaxDepth + 2][3];
   float s_mind[kMaxDepth + 2];
-#endif
   unsigned visits = 0, ver = 0;
   for (;;) {
     ++visits;
@@ -196,13 +214,6 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
       const float o0 = dim == 0 ? fmaxf(t, off[0]) : off[0];
       const float o1 = dim == 1 ? fmaxf(t, off[1]) : off[1];
       const float o2 = dim == 2 ? fmaxf(t, off[2]) : off[2];
-#if VT_STACK_NM
-      const float nm = fmaxf(__fadd_rn(__fadd_rn(o0, o1), o2), base);
-      if (nm < thr32) {
-        s_e[sp] = make_int2(other, __float_as_int(nm));
-        ++sp;
-      }
-#else
       const float nm = __fadd_rn(__fadd_rn(o0, o1), o2);
       if (nm < thr32) {
         s_node[sp] = other;
@@ -212,19 +223,34 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
         s_off[sp][2] = o2;
         ++sp;
       }
-#endif
       node = best;
       continue;
     }
     {
       int64_t a, b;
       leaf_range(c, node - ninternal, a, b);
+#if VT_LEAF_BATCH
+      // the FP32 distances of up to VT_LEAF_BATCH points first (independent
+      // loads in flight together), then the tests in point order
+      for (int64_t p0 = a; p0 < b; p0 += VT_LEAF_BATCH) {
+        float fb[VT_LEAF_BATCH];
+#pragma unroll
+        for (int j = 0; j < VT_LEAF_BATCH; ++j) {
+          fb[j] = __int_as_float(0x7f800000);
+          if (p0 + j < b) fb[j] = pt_dist32(q0, q1, q2, __ldg(&c.pts32[p0 + j]));
+        }
+#pragma unroll
+        for (int j = 0; j < VT_LEAF_BATCH; ++j) {
+        const int64_t p = p0 + j;
+        const float f = fb[j];
+#else
       for (int64_t p = a; p < b; ++p) {
         const float4 P = __ldg(&c.pts32[p]);
         const float d0 = __fsub_rn(q0, P.x), d1 = __fsub_rn(q1, P.y),
                     d2 = __fsub_rn(q2, P.z);
         const float f =
             __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
+#endif
         if (f < thr32) {
           const int pi = (int)p;
           double d;
@@ -241,20 +267,13 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
           }
         }
       }
+#if VT_LEAF_BATCH
+      }
+#endif
     }
     bool found = false;
     while (sp > 0) {
       --sp;
-#if VT_STACK_NM
-      const int2 e = s_e[sp];
-      if (__int_as_float(e.y) < thr32) {
-        node = e.x;
-        base = __int_as_float(e.y);
-        off[0] = off[1] = off[2] = 0.f;
-        found = true;
-        break;
-      }
-#else
       if (s_mind[sp] < thr32) {
         node = s_node[sp];
         off[0] = s_off[sp][0];
@@ -263,7 +282,6 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
         found = true;
         break;
       }
-#endif
     }
     if (!found) break;
   }
@@ -384,7 +402,7 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
   st.clear();
   double q_err = 0.0;
   // sinks
-  std::conditional_t<OUT == kOutTape, TapeReducer<MODE, NF>, Reducer<MODE, NF>> red;
+  std::conditional_t<OUT == kOutTape, TapeReducer<MODE, NF, true>, Reducer<MODE, NF>> red;
   FillSink fill;
   AdjSink<MODE, NF> adj;
   // lane counters
@@ -615,6 +633,8 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
         }
       }
     }
+    // every lane reaches the end of a trip: write this trip's tape entries
+    if constexpr (OUT == kOutTape) red.flush_tape(io);
   }
   warp_add(&io.stats->rays, n_rays);
   warp_add(&io.stats->crossings, n_cross);

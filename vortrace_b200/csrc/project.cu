@@ -106,41 +106,74 @@ struct Reducer {
 // Append one tape entry; the lanes of a warp that reach this point together
 // reserve their slots with one atomic.  Entries past tape_cap are counted
 // but not written (the host then sizes the tape from the count).
+// Append one tape entry from one lane (its own slot).  Entries past
+// tape_cap are counted but not written (the host then sizes the tape from
+// the count).
 template <class E>
 __device__ __forceinline__ void tape_append(const WalkIO& io, const E& e) {
-  const unsigned m = __activemask();
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(m) - 1;
-  unsigned long long base = 0;
-  if (lane == leader) base = atomicAdd(io.tape_count, (unsigned long long)__popc(m));
-  base = __shfl_sync(m, base, leader);
-  const unsigned long long k = base + __popc(m & ((1u << lane) - 1u));
+  const unsigned long long k = atomicAdd(io.tape_count, 1ULL);
   if (k < io.tape_cap) static_cast<E*>(io.tape)[k] = e;
 }
 
 // Reducer of 'integrate' or 'volume' that also records the tape; the first
 // `skip` segments of the ray were recorded by an earlier, handed-over launch.
-template <int MODE, int NF>
+// STAGED (the batched thread kernel): the segments of one loop trip (at most
+// two) wait in registers and flush_tape, which every lane of the warp calls
+// at the end of each trip, writes them with one atomic per warp; otherwise
+// each segment takes its own slot.
+template <int MODE, int NF, bool STAGED = false>
 struct TapeReducer : Reducer<MODE, NF> {
+  using E = typename std::conditional<MODE == kVolume, TapeEntryV, TapeEntry>::type;
   const WalkIO* io;
   int ray;
   unsigned skip;
+  int npend = 0;
+  E pend[2];
   __device__ __forceinline__ void set_tape(const WalkIO* w, int64_t r, unsigned sk) {
     io = w;
     ray = (int)r;
     skip = sk;
   }
+  __device__ __forceinline__ void record(const E& e) {
+    if (STAGED) {
+      if (npend == 0) pend[0] = e;
+      else pend[1] = e;
+      ++npend;
+    } else {
+      tape_append(*io, e);
+    }
+  }
   __device__ __forceinline__ void seg(int cell, double a, double b) {
-    if (MODE == kVolume) {
+    if constexpr (MODE == kVolume) {
       const double T0 = this->T;
       Reducer<MODE, NF>::seg(cell, a, b);
       if (this->nseg > skip)
-        tape_append(*io, TapeEntryV{cell, ray, dsub(b, a), T0,
-                                    {this->acc[0], this->acc[1], this->acc[2]}});
+        record(TapeEntryV{cell, ray, dsub(b, a), T0, {this->acc[0], this->acc[1], this->acc[2]}});
     } else {
       Reducer<MODE, NF>::seg(cell, a, b);
-      if (this->nseg > skip) tape_append(*io, TapeEntry{this->c->perm[cell], ray, dsub(b, a)});
+      if (this->nseg > skip) record(TapeEntry{this->c->perm[cell], ray, dsub(b, a)});
     }
+  }
+  // all 32 lanes: write the staged entries (warp prefix sum, one atomic)
+  __device__ __forceinline__ void flush_tape(const WalkIO& w) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int incl = npend;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(full, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(full, incl, 31);
+    if (total == 0) return;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(w.tape_count, (unsigned long long)total);
+    base = __shfl_sync(full, base, 0);
+    const unsigned long long k = base + (unsigned long long)(incl - npend);
+    E* t = static_cast<E*>(w.tape);
+    if (npend > 0 && k < w.tape_cap) t[k] = pend[0];
+    if (npend > 1 && k + 1 < w.tape_cap) t[k + 1] = pend[1];
+    npend = 0;
   }
 };
 
