@@ -49,10 +49,11 @@ UNIT = "Mcrossings/s"
 BX = {"clustered_2m": 3262.25, "uniform_100k": 2915.74}
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per crossing of
-# the AUTO kernel, from one ncu capture of the 512x512 case of clustered_2m
-# (profiles/k_batched_fp32_clustered_2m_npix512.md: 3.79 GB for 49,726,019
-# crossings); the full-size launch is taken to scale with its crossings.
-DRAM_BYTES_PER_CROSSING = {"clustered_2m": 76.2}
+# the guarded-FP32 kernel, from one ncu capture of the 512x512 case of
+# clustered_2m (profiles/k_batched_fp32_clustered_2m_npix512.md: 4.35 GB for
+# 49,726,019 crossings); the full-size launch is taken to scale with its
+# crossings.
+DRAM_BYTES_PER_CROSSING = {"clustered_2m": 87.5}
 
 
 def dist_env():
