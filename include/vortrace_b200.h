@@ -187,6 +187,23 @@ int vt_project_device(vt_cloud *cloud, const double *d_starts, const double *d_e
 int vt_project_device_noalloc(vt_cloud *cloud, const double *d_starts, const double *d_ends,
                               uint64_t nrays, int mode, double *d_out, void *stream);
 
+/* The rays of an unrotated projection grid, generated on the device
+ * (replaces generate_projection_grid with center=None, vortrace/grid.py:35-44
+ * and :100-192, on the host).  extent = {x0, x1, y0, y1}; nx x ny pixels;
+ * ray i*ny + j runs from (x_i, y_j, bounds[0]) to (x_i, y_j, bounds[1]), x_i
+ * and y_j the pixel centres numpy.linspace gives the reference's generator,
+ * bit for bit.  d_starts / d_ends hold nx*ny*3 doubles; enqueued on `stream`
+ * (a cudaStream_t) without synchronising. */
+int vt_grid_rays_device(const double extent[4], uint64_t nx, uint64_t ny,
+                        const double bounds[2], double *d_starts, double *d_ends, void *stream);
+/* grid_projection with center=None (vortrace/vortrace.py:141-195): the grid's
+ * rays generated on the device (vt_grid_rays_device) and projected as by
+ * vt_project; out holds nx*ny*nout values, ray i*ny + j.  No ray crosses the
+ * host-device link. */
+int vt_project_grid(vt_cloud *cloud, const double extent[4], uint64_t nx, uint64_t ny,
+                    const double bounds[2], int mode, int kernel, double *out,
+                    vt_stats *stats);
+
 /* makeDetailedProjection + returnSegments (src/projection.cpp:75-144,
  * src/bindings.cpp:206-238).  Writes out (as vt_project) and the CSR
  * offsets (nrays + 1 entries), and returns a library-owned segment list

@@ -47,7 +47,7 @@ EXPORTS = (
     "vt_tape_create", "vt_tape_destroy", "vt_tape_size", "vt_project_device_tape",
     "vt_tape_adjoint_device", "vt_slice", "vt_brute_projection", "vt_cloud_autotune",
     "vt_graph_create", "vt_graph_launch", "vt_graph_finish", "vt_graph_destroy",
-    "vt_cloud_tree_save", "vt_cloud_tree_load",
+    "vt_cloud_tree_save", "vt_cloud_tree_load", "vt_grid_rays_device", "vt_project_grid",
 )
 
 
@@ -153,6 +153,9 @@ def load(path: str | None = None):
         L.vt_graph_destroy.argtypes = [vp]
         L.vt_graph_destroy.restype = None
         L.vt_brute_projection.argtypes = [vp, C.POINTER(u64), dp, C.c_int, dp]
+        L.vt_grid_rays_device.argtypes = [dp, u64, u64, dp, vp, vp, vp]
+        L.vt_project_grid.argtypes = [vp, dp, u64, u64, dp, C.c_int, C.c_int, dp,
+                                      C.POINTER(Stats)]
         L.vt_tape_size.argtypes = [vp]
         L.vt_tape_size.restype = u64
         L.vt_project_device_tape.argtypes = [vp, vp, vp, vp, u64, C.c_int, C.c_int, vp, vp,
@@ -167,7 +170,8 @@ def load(path: str | None = None):
                      "vt_tape_create", "vt_project_device_tape", "vt_tape_adjoint_device",
                      "vt_slice", "vt_brute_projection", "vt_cloud_autotune",
                      "vt_graph_create", "vt_graph_launch", "vt_graph_finish",
-                     "vt_cloud_tree_save", "vt_cloud_tree_load"):
+                     "vt_cloud_tree_save", "vt_cloud_tree_load", "vt_grid_rays_device",
+                     "vt_project_grid"):
             getattr(L, name).restype = C.c_int
         L.vt_set_warning_callback(_warn_cb)
         _lib = L

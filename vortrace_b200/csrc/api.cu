@@ -502,6 +502,59 @@ int vt_project(vt_cloud* cl, const double* starts, const double* ends, uint64_t 
   VT_GUARD_END
 }
 
+static int check_grid_args(const double* extent, uint64_t nx, uint64_t ny,
+                           const double* bounds) {
+  if (!extent || !bounds) return set_error(VT_ERR_INVALID, "null argument");
+  if (nx == 0 || ny == 0) return set_error(VT_ERR_INVALID, "grid resolution must be positive");
+  if (nx > (uint64_t)1 << 31 || ny > (uint64_t)1 << 31 || nx * ny > (uint64_t)1 << 40)
+    return set_error(VT_ERR_INVALID, "grid resolution too large");
+  for (int i = 0; i < 4; ++i)
+    if (!std::isfinite(extent[i])) return set_error(VT_ERR_INVALID, "extent must be finite");
+  if (!std::isfinite(bounds[0]) || !std::isfinite(bounds[1]))
+    return set_error(VT_ERR_INVALID, "bounds must be finite");
+  return VT_OK;
+}
+
+int vt_grid_rays_device(const double extent[4], uint64_t nx, uint64_t ny,
+                        const double bounds[2], double* d_starts, double* d_ends, void* stream) {
+  VT_GUARD_BEGIN
+  int rc = check_grid_args(extent, nx, ny, bounds);
+  if (rc) return rc;
+  if (!d_starts || !d_ends) return set_error(VT_ERR_INVALID, "null argument");
+  return vt::launch_grid_rays(extent, nx, ny, bounds, d_starts, d_ends,
+                              (cudaStream_t)stream);
+  VT_GUARD_END
+}
+
+int vt_project_grid(vt_cloud* cl, const double extent[4], uint64_t nx, uint64_t ny,
+                    const double bounds[2], int mode, int kernel, double* out,
+                    vt_stats* stats) {
+  VT_GUARD_BEGIN
+  int rc = check_projectable(cl, mode);
+  if (rc) return rc;
+  if ((rc = check_grid_args(extent, nx, ny, bounds))) return rc;
+  if (!out) return set_error(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  VT_CUDA(cudaSetDevice(cl->device));
+  if (stats) memset(stats, 0, sizeof(*stats));
+  const uint64_t nrays = nx * ny;
+  const int nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
+  if ((rc = cl->ws_starts.reserve(3 * nrays)) || (rc = cl->ws_ends.reserve(3 * nrays)) ||
+      (rc = cl->ws_out.reserve(nrays * nout)))
+    return rc;
+  cudaStream_t st = cl->stream;
+  if ((rc = vt::launch_grid_rays(extent, nx, ny, bounds, cl->ws_starts.p, cl->ws_ends.p, st)))
+    return rc;
+  rc = project_device_locked(cl, cl->ws_starts.p, cl->ws_ends.p, nrays, mode, kernel,
+                             cl->ws_out.p, st, stats, vt::kOutImage, nullptr);
+  if (rc) return rc;
+  VT_CUDA(cudaMemcpyAsync(out, cl->ws_out.p, nrays * nout * sizeof(double),
+                          cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  return VT_OK;
+  VT_GUARD_END
+}
+
 int vt_project_detailed(vt_cloud* cl, const double* starts, const double* ends, uint64_t nrays,
                         int mode, double* out, int64_t* offsets, vt_segments** segs) {
   VT_GUARD_BEGIN

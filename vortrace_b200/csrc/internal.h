@@ -159,4 +159,7 @@ int upload_fields(vt_cloud* cl, const double* src, bool src_device, cudaStream_t
 int check_projectable(const vt_cloud* cl, int mode);
 // the kernel VT_KERNEL_AUTO stands for with this cloud and batch size
 int resolve_kernel(const vt_cloud* cl, int kernel, uint64_t nrays);
+// pixel-centre z-grid rays on the device (grid.cu), ray i*ny + j
+int launch_grid_rays(const double extent[4], uint64_t nx, uint64_t ny, const double bounds[2],
+                     double* d_starts, double* d_ends, cudaStream_t st);
 }

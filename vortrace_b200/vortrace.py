@@ -263,6 +263,10 @@ class ProjectionCloud:
                         roll=0.0, reduction="integrate") -> np.ndarray:
         """Grid projection; see the reference (vortrace/vortrace.py:141-195)."""
         mode = self._validate_reduction(reduction)
+        if center is None:
+            dev = self._device_grid_projection(extent, nres, bounds, proj, mode)
+            if dev is not None:
+                return dev
         ps, pe = gr.generate_projection_grid(extent, nres, bounds, center, proj=proj, yaw=yaw,
                                              pitch=pitch, roll=roll)
         shape = ps.shape
@@ -273,6 +277,35 @@ class ProjectionCloud:
         if nout == 1:
             return np.reshape(dat, shape[:-1])
         return np.reshape(dat, (*shape[:-1], nout))
+
+    def _device_grid_projection(self, extent, nres, bounds, proj, mode):
+        """An unrotated grid's projection with its rays generated on the device
+        (vt_project_grid); None where the host generator must run instead
+        (an extent whose dtype makes numpy compute the pixel centres in
+        another precision)."""
+        ext = np.asarray(extent)
+        if not (ext.dtype == np.float64 or ext.dtype.kind in "iu"):
+            return None
+        ext = gr._as_extent(ext).astype(np.float64)
+        nx, ny = gr._as_nres(nres)
+        b = np.asarray(bounds, dtype=np.float64).ravel()
+        if nx <= 0 or ny <= 0 or b.size != 2 or ext.shape != (2, 2):
+            return None  # the host generator raises the reference's errors
+        # bounds flip of generate_projection_grid (vortrace/grid.py:163-172)
+        hand = gr.projection_angles(proj)[3] if proj is not None else np.sign(b[1] - b[0])
+        if hand != np.sign(b[1] - b[0]):
+            b = b[::-1].copy()
+        e4 = np.ascontiguousarray([ext[0][0], ext[0][1], ext[1][0], ext[1][1]], np.float64)
+        nout = self._nout(mode)
+        out = np.empty((nx * ny, nout), np.float64)
+        st = L.Stats()
+        cl = self._cloud
+        L.check(cl._lib.vt_project_grid(cl._h, L.dptr(e4), nx, ny, L.dptr(b), mode,
+                                        L.KERNELS[self.kernel], L.dptr(out), C.byref(st)))
+        self.last_stats = st.as_dict()
+        if nout == 1:
+            return out.reshape(nx, ny)
+        return out.reshape(nx, ny, nout)
 
     def projection(self, pos_start, pos_end, *, reduction="integrate") -> np.ndarray:
         """Projection of arbitrary rays (vortrace/vortrace.py:197-227)."""
