@@ -94,3 +94,34 @@ def test_grid_projection_float32_extent_uses_host_rays(cloud):
     hs, he = gr.generate_projection_grid(ext, 64, [0.0, 100.0], None)
     ref = cloud.projection(hs.reshape(-1, 3), he.reshape(-1, 3), reduction="max")
     assert np.array_equal(img.reshape(-1, 2), ref)
+
+
+@pytest.mark.parametrize("reduction", ["integrate", "volume"])
+def test_autograd_grid_project_device_rays(reduction):
+    """autograd.grid_project with center=None takes its rays from the device
+    generator: same image bits and gradient as projecting the host rays."""
+    import torch
+    from vortrace_b200 import autograd as VA
+    rng = np.random.default_rng(5)
+    n = 20000
+    pos = rng.uniform(0.0, 100.0, (n, 3))
+    if reduction == "volume":
+        f = np.column_stack([rng.uniform(0, 1, (n, 3)), rng.uniform(0.0, 0.2, n)])
+    else:
+        f = np.column_stack([rng.lognormal(0.0, 1.0, n), rng.uniform(0.0, 1.0, n)])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        pc = vt.ProjectionCloud(pos, f, boundbox=[0.0, 100.0] * 3)
+    ft = torch.tensor(f, device="cuda", requires_grad=True)
+    img = VA.grid_project(pc, ft, [[10, 90], [20, 80]], (48, 40), [0, 100], None,
+                          reduction=reduction)
+    w = torch.as_tensor(rng.normal(size=tuple(img.shape)), device="cuda")
+    (img * w).sum().backward()
+    g_dev = ft.grad.clone()
+    ft.grad = None
+    hs, he = gr.generate_projection_grid([[10, 90], [20, 80]], (48, 40), [0, 100], None)
+    ref = VA.project(pc, ft, hs.reshape(-1, 3), he.reshape(-1, 3), reduction=reduction)
+    assert img.shape[:2] == (48, 40)
+    assert torch.equal(img.reshape(ref.shape), ref)
+    (ref * w.reshape(ref.shape)).sum().backward()
+    torch.testing.assert_close(g_dev, ft.grad, rtol=1e-12, atol=1e-15)

@@ -99,6 +99,15 @@ class _ProjectFn(torch.autograd.Function):
         return grad, None, None, None, None, None
 
 
+def _rays_on(p, dev) -> torch.Tensor:
+    """(R, 3) float64 rays on ``dev``: device tensors are used in place,
+    host arrays copied once."""
+    if isinstance(p, torch.Tensor):
+        return p.to(device=dev, dtype=torch.float64).reshape(-1, 3).contiguous()
+    a = np.ascontiguousarray(p, np.float64)
+    return torch.as_tensor(a, device=dev).reshape(-1, 3).contiguous()
+
+
 def project(pc: ProjectionCloud, fields: torch.Tensor, pos_start, pos_end, *,
             reduction: str = "integrate", kernel: str = "auto") -> torch.Tensor:
     """Differentiable :meth:`ProjectionCloud.projection`.
@@ -106,7 +115,8 @@ def project(pc: ProjectionCloud, fields: torch.Tensor, pos_start, pos_end, *,
     ``fields``: tensor of shape (N,) or (N, nfields) over the ORIGINAL
     particles (the order of ``pos`` given to the cloud); only the particles
     kept by the bounding-box filter influence the result.  ``pos_start`` /
-    ``pos_end``: (R, 3) rays.  Returns (R,) or (R, nout) float64 on the
+    ``pos_end``: (R, 3) rays, host arrays or tensors (device tensors are used
+    without a copy).  Returns (R,) or (R, nout) float64 on the
     device of ``fields`` (must be a CUDA tensor).
     """
     mode = {"integrate": L.REDUCE_SUM, "sum": L.REDUCE_SUM, "volume": L.REDUCE_VOLUME,
@@ -126,9 +136,8 @@ def project(pc: ProjectionCloud, fields: torch.Tensor, pos_start, pos_end, *,
                          f"(R, G, B, alpha), got {pc._nfields}")
     oid = torch.as_tensor(pc.orig_ids, device=dev, dtype=torch.long)
     fi = f2.index_select(0, oid)
-    S = torch.as_tensor(np.ascontiguousarray(pos_start, np.float64), device=dev).reshape(-1, 3)
-    E = torch.as_tensor(np.ascontiguousarray(pos_end, np.float64), device=dev).reshape(-1, 3)
-    out = _ProjectFn.apply(fi, pc, S.contiguous(), E.contiguous(), mode, L.KERNELS[kernel])
+    S, E = (_rays_on(p, dev) for p in (pos_start, pos_end))
+    out = _ProjectFn.apply(fi, pc, S, E, mode, L.KERNELS[kernel])
     return out[:, 0] if (out.shape[1] == 1 and fields.dim() == 1) else out
 
 
@@ -136,7 +145,24 @@ def grid_project(pc: ProjectionCloud, fields: torch.Tensor, extent, nres, bounds
                  reduction: str = "integrate", **angles) -> torch.Tensor:
     """Differentiable :meth:`ProjectionCloud.grid_projection`."""
     from . import grid as gr
-    ps, pe = gr.generate_projection_grid(extent, nres, bounds, center, **angles)
-    shape = ps.shape[:-1]
-    out = project(pc, fields, ps.reshape(-1, 3), pe.reshape(-1, 3), reduction=reduction)
+    from .vortrace import device_grid_args
+    args = None
+    if center is None and fields.is_cuda:
+        args = device_grid_args(extent, nres, bounds, angles.get("proj"))
+    if args is not None:
+        # the unrotated grid's rays made on the device (vt_grid_rays_device)
+        e4, nx, ny, b = args
+        dev = fields.device
+        ps = torch.empty((nx * ny, 3), dtype=torch.float64, device=dev)
+        pe = torch.empty_like(ps)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        with torch.cuda.device(dev):
+            L.check(pc._cloud._lib.vt_grid_rays_device(L.dptr(e4), nx, ny, L.dptr(b),
+                                                       _dev_ptr(ps), _dev_ptr(pe), stream))
+        shape = (nx, ny)
+    else:
+        ps, pe = gr.generate_projection_grid(extent, nres, bounds, center, **angles)
+        shape = ps.shape[:-1]
+        ps, pe = ps.reshape(-1, 3), pe.reshape(-1, 3)
+    out = project(pc, fields, ps, pe, reduction=reduction)
     return out.reshape(*shape, *out.shape[1:])

@@ -41,6 +41,12 @@ constexpr int kBatchStack = 32;
 #ifndef VT_LEAF_BATCH64
 #define VT_LEAF_BATCH64 4
 #endif
+// 1: the launch statistics also count the tree nodes the searches visit
+// (search_steps) and the FP64 re-checks of FP32-passing points
+// (fp64_checks); off by default, the counters cost registers
+#ifndef VT_BATCHED_COUNTERS
+#define VT_BATCHED_COUNTERS 0
+#endif
 
 // ---- node fetch (shared memory for the top levels) ----------------------
 struct Fetch64 {
@@ -184,7 +190,22 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
   res.clear();
   double thr64 = R;
   float thr32 = __double2float_ru(dadd(thr64, G));
-  float off[3] = {0.f, 0.f, 0.f};
+  // per-axis offsets start at the squared distance to the cloud's box
+  // (nanoflann's computeInitialDistances, include/nanoflann.hpp:1005-1022):
+  // a query outside the box (rays that start or end outside the cloud)
+  // prunes with it.  bblo32/bbhi32 are rounded outward and the offsets
+  // rounded down, so they stay below every point's FP32 offset.
+  float off[3];
+  {
+    const float qd[3] = {q0, q1, q2};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float t = 0.f;
+      if (qd[d] < c.bblo32[d]) t = __fsub_rd(c.bblo32[d], qd[d]);
+      else if (qd[d] > c.bbhi32[d]) t = __fsub_rd(qd[d], c.bbhi32[d]);
+      off[d] = __fmul_rd(t, t);
+    }
+  }
   const int64_t ninternal = c.nleaves - 1;
   int node = 0;
   int sp = 0;
@@ -641,6 +662,10 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
   warp_add(&io.stats->queries, n_q);
   warp_add(&io.stats->fp64_resolves, n_res);
   warp_max(&io.stats->max_stack, max_sp);
+#if VT_BATCHED_COUNTERS
+  warp_add(&io.stats->pad[0], n_visit);
+  warp_add(&io.stats->pad[1], n_ver);
+#endif
 }
 
 template <int MODE, int NF, int OUT>

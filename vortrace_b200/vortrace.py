@@ -189,6 +189,31 @@ def _as_values(out, nout):
     return out[:, 0].copy() if nout == 1 else out
 
 
+def device_grid_args(extent, nres, bounds, proj=None):
+    """Arguments of vt_project_grid / vt_grid_rays_device for an unrotated
+    grid: ``(extent4, nx, ny, bounds2)`` with the bounds flip of
+    generate_projection_grid applied (vortrace/grid.py:163-172), or None
+    where the host generator must run instead: an extent whose dtype makes
+    numpy compute the pixel centres in another precision (float32), or
+    arguments the host generator rejects with the reference's errors."""
+    ext = np.asarray(extent)
+    if not (ext.dtype == np.float64 or ext.dtype.kind in "iu"):
+        return None
+    try:
+        ext = gr._as_extent(ext).astype(np.float64)
+        nx, ny = gr._as_nres(nres)
+        b = np.asarray(bounds, dtype=np.float64).ravel()
+    except (ValueError, TypeError):
+        return None
+    if nx <= 0 or ny <= 0 or b.size != 2 or ext.shape != (2, 2):
+        return None
+    hand = gr.projection_angles(proj)[3] if proj is not None else np.sign(b[1] - b[0])
+    if hand != np.sign(b[1] - b[0]):
+        b = b[::-1].copy()
+    e4 = np.ascontiguousarray([ext[0][0], ext[0][1], ext[1][0], ext[1][1]], np.float64)
+    return e4, nx, ny, np.ascontiguousarray(b)
+
+
 class ProjectionCloud:
     """Projections through an unstructured Voronoi mesh on a B200.
 
@@ -280,22 +305,11 @@ class ProjectionCloud:
 
     def _device_grid_projection(self, extent, nres, bounds, proj, mode):
         """An unrotated grid's projection with its rays generated on the device
-        (vt_project_grid); None where the host generator must run instead
-        (an extent whose dtype makes numpy compute the pixel centres in
-        another precision)."""
-        ext = np.asarray(extent)
-        if not (ext.dtype == np.float64 or ext.dtype.kind in "iu"):
+        (vt_project_grid); None where the host generator must run instead."""
+        args = device_grid_args(extent, nres, bounds, proj)
+        if args is None:
             return None
-        ext = gr._as_extent(ext).astype(np.float64)
-        nx, ny = gr._as_nres(nres)
-        b = np.asarray(bounds, dtype=np.float64).ravel()
-        if nx <= 0 or ny <= 0 or b.size != 2 or ext.shape != (2, 2):
-            return None  # the host generator raises the reference's errors
-        # bounds flip of generate_projection_grid (vortrace/grid.py:163-172)
-        hand = gr.projection_angles(proj)[3] if proj is not None else np.sign(b[1] - b[0])
-        if hand != np.sign(b[1] - b[0]):
-            b = b[::-1].copy()
-        e4 = np.ascontiguousarray([ext[0][0], ext[0][1], ext[1][0], ext[1][1]], np.float64)
+        e4, nx, ny, b = args
         nout = self._nout(mode)
         out = np.empty((nx * ny, nout), np.float64)
         st = L.Stats()
