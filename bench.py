@@ -46,7 +46,8 @@ METRIC = "Mcrossings/s fwd & fwd+bwd: batched guarded-FP32 vs plain FP64 GPU ker
 UNIT = "Mcrossings/s"
 # Algorithmic bytes per cell crossing, B_x = Q*(n_node*16 + n_pt*24) + nf*8 + 48,
 # measured with the nanoflann restatement (oracle/measure_bx.py, 8192-ray sample).
-BX = {"clustered_2m": 3262.25, "uniform_100k": 2915.74}
+BX = {"clustered_2m": 3262.25, "uniform_100k": 2915.74, "volume_2m": 3273.36,
+      "batched_1m": 3201.12, "nested_16m": 3320.48}
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per crossing of
 # the guarded-FP32 kernel, from one ncu capture of the 512x512 case of
