@@ -346,7 +346,7 @@ struct RareOut {
 };
 
 // Parallel-bisector fallback of the split point (src/ray.cpp:96-126).
-__device__ __noinline__ RareOut rare_split(const DevCloud& c, RayGeom g, int cur, int nxt,
+static __device__ __noinline__ RareOut rare_split(const DevCloud& c, RayGeom g, int cur, int nxt,
                                            double cur_s, double nxt_s) {
   Search64 S(c);
   RareOut o{0.0, 0, 0, 0, 0u};
@@ -356,7 +356,7 @@ __device__ __noinline__ RareOut rare_split(const DevCloud& c, RayGeom g, int cur
 }
 
 // Case 1a (src/ray.cpp:364-422): intermediate cells on both sides.
-__device__ __noinline__ RareOut rare_case1a(const DevCloud& c, RayGeom g, double x, double y,
+static __device__ __noinline__ RareOut rare_case1a(const DevCloud& c, RayGeom g, double x, double y,
                                             double z, int cur, int nxt) {
   Search64 S(c);
   int sc = try_along_ray(g, S, x, y, z, -1.0, cur, nxt);
@@ -379,7 +379,7 @@ __device__ __noinline__ RareOut rare_case1a(const DevCloud& c, RayGeom g, double
 }
 
 // 100-NN classification (src/ray.cpp:319-338).
-__device__ __noinline__ RareOut rare_expand(const DevCloud& c, double x, double y, double z,
+static __device__ __noinline__ RareOut rare_expand(const DevCloud& c, double x, double y, double z,
                                             int cur, int nxt) {
   bool has_c = false, has_n = false;
   unsigned v = 0;

@@ -69,4 +69,16 @@ struct WalkIO {
 int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaStream_t st,
              vt_stats* stats);
 
+// Launchers of the walk kernels, one translation unit each (walk_*.cu):
+// image / count (segments per ray) of 'integrate' and of the other
+// reductions, CSR fill, taped forward ('integrate' or 'volume') and the
+// re-walk adjoint ('integrate' or 'volume').
+int launch_image_sum(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st);
+int launch_image_vmm(vt_cloud* cl, WalkIO& io, int mode, int kernel, cudaStream_t st);
+int launch_count_sum(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st);
+int launch_count_vmm(vt_cloud* cl, WalkIO& io, int mode, int kernel, cudaStream_t st);
+int launch_fill(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st);
+int launch_tape(vt_cloud* cl, WalkIO& io, int mode, int kernel, cudaStream_t st);
+int launch_adj(vt_cloud* cl, WalkIO& io, int mode, int kernel, cudaStream_t st);
+
 }  // namespace vt
