@@ -43,6 +43,8 @@ extern "C" {
 #define VT_ERR_STACK 15        /* pending-point stack above VT_PARAM_STACK_CAP
                                   (the reference's list is heap-grown)         */
 #define VT_ERR_PERIODIC_BISECT 18 /* src/ray.cpp:243-246 periodic same-cell ray */
+#define VT_ERR_TIE 19          /* an exact distance tie could not be resolved
+                                  in the reference's order (no counterpart) */
 
 /* ---- reduction modes: include/mytypes.hpp:14 (ReductionMode) ----------- */
 #define VT_REDUCE_SUM 0
@@ -77,6 +79,8 @@ extern "C" {
                                   /* cache of the split-point queries (1, 0)   */
 #define VT_PARAM_ADJOINT_KERNEL 9 /* walk kernel of the re-walk adjoint        */
                                   /* (VT_KERNEL_*; default AUTO)               */
+#define VT_PARAM_DETAILED_KERNEL 10 /* walk kernel of vt_project_detailed      */
+                                    /* (VT_KERNEL_*; default AUTO)             */
 
 typedef struct vt_cloud vt_cloud;
 typedef struct vt_segments vt_segments;
@@ -95,6 +99,10 @@ typedef struct {
   uint64_t tree_leaves;
   double tree_build_ms;
   uint64_t device_bytes; /* device memory held by the handle                */
+  uint64_t tie_tree_nodes; /* reference-order tree: nodes (0: not built)    */
+  int32_t tie_tree_depth;  /* ... its depth in nodes                        */
+  int32_t reserved;
+  double tie_tree_build_ms;
 } vt_cloud_info;
 
 typedef struct {
@@ -109,6 +117,8 @@ typedef struct {
   uint64_t fp64_checks;   /* FP64 re-checks of points passing the FP32 test  */
   uint64_t cache_refreshes; /* neighbourhood-cache refills (batched kernel)  */
   uint64_t cache_hits;    /* split queries answered from the cache           */
+  uint64_t ties;          /* 1-NN queries whose nearest distance was exactly
+                             shared, answered in the reference's order       */
 } vt_stats;
 
 /* ---- library ----------------------------------------------------------- */
@@ -152,9 +162,26 @@ void vt_cloud_destroy(vt_cloud *cloud);
 /* PointCloud::queryTree(q, k) (src/bindings.cpp:155-174): exact k-NN of nq
  * query points (host buffers); ids are internal (filtered) indices, r2 the
  * squared distances in the reference's summation order.  Missing entries
- * (k > npart) get id -1 and r2 = DBL_MAX. */
+ * (k > npart) get id -1 and r2 = DBL_MAX.  Exactly tied distances come in
+ * the reference's order (the queries are repeated on the reference-order
+ * tree when a tie is seen, see vt_cloud_build_tie_tree). */
 int vt_knn(const vt_cloud *cloud, const double *q, uint64_t nq, int k, int64_t *ids,
            double *r2);
+
+/* The reference-order tree: nanoflann's middle-split k-d tree (the
+ * reference's PointCloud::buildTree, src/pointcloud.cpp:193-212, over
+ * include/nanoflann.hpp:858-1003) built on the host and kept on the device
+ * beside the device tree.  The device tree answers every query; when the
+ * nearest distance of a 1-NN query (ray ends, bisection, perturbation,
+ * Slice, BruteProjection) or the order of a k-NN list depends on exactly
+ * tied generators (lattices, quantised positions, rays along faces), the
+ * query is repeated on this tree so that the tie resolves as in the
+ * reference.  Projections build it on first need (and finish the affected
+ * rays after it); this call builds it ahead, e.g. before
+ * vt_project_device_noalloc, which never allocates and fails with
+ * VT_ERR_RUNTIME on a tie while the tree is missing.  Rebuilding or
+ * reloading the device tree drops it. */
+int vt_cloud_build_tie_tree(vt_cloud *cloud);
 
 /* ---- projections ------------------------------------------------------- */
 /* Projection(starts, ends) + makeProjection(cloud, mode) + returnProjection
@@ -174,16 +201,23 @@ int vt_project_device(vt_cloud *cloud, const double *d_starts, const double *d_e
  * project: a framework whose caching allocator owns the device pool, or a
  * latency-critical loop that cannot afford cudaMalloc/cudaFree and their
  * implicit synchronisation.  Inputs and outputs are the caller's device
- * buffers (starts/ends nrays x 3, out nrays x nout; kernel: the batched
- * one); the walk's scratch is a fixed 8.9 MB static device array that every
- * GPU loading the library holds until exit.  Limits: at most 1,048,576 rays
- * per call (larger requests fail with VT_ERR_INVALID) and 512 pending ray
+ * buffers (starts/ends nrays x 3, out nrays x nout).  The walk kernel is
+ * fixed: one warp per ray (VT_KERNEL_BATCHED) in the caller's ray order,
+ * because the coherent ray sort of the other batched kernel needs scratch
+ * that grows with the batch.  The walk's scratch is a fixed 8.9 MB static
+ * device array, placed on a device when the library's device code is first
+ * loaded there (with lazy module loading: by the first projection call on
+ * that device) and held until exit.  Limits: at most 1,048,576 rays per
+ * call (larger requests fail with VT_ERR_INVALID) and 512 pending ray
  * points for rays handed to the global-stack kernel (VT_ERR_STACK beyond).
- * The first call on a device looks up the scratch's device address; make
- * that first call before any stream capture.  All calls share the one
- * scratch array: calls that overlap on the GPU (other streams, other
- * threads, other handles on the same device) race and must be serialised
- * by the caller.  Returns after the launch has completed. */
+ * An exact distance tie needs the reference-order tree, which this call
+ * never builds: it fails with VT_ERR_RUNTIME until vt_cloud_build_tie_tree
+ * has been called on the handle.  The first call on a device looks up the
+ * scratch's device address; make that first call before any stream
+ * capture.  All calls share the one scratch array: calls that overlap on
+ * the GPU (other streams, other threads, other handles on the same device)
+ * race and must be serialised by the caller.  The call synchronises
+ * `stream` and returns after the launch has completed. */
 int vt_project_device_noalloc(vt_cloud *cloud, const double *d_starts, const double *d_ends,
                               uint64_t nrays, int mode, double *d_out, void *stream);
 

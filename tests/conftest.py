@@ -38,6 +38,19 @@ def small_walks():
 
 
 @pytest.fixture(scope="session")
+def tie_walks():
+    """Exact-tie geometry produced by the reference module: segment lists of
+    lattice clouds, k-NN order of tied generators, Slice/BruteProjection
+    samples on lattice faces (tests/golden/make_golden.py, ``ties``)."""
+    z = np.load(os.path.join(GOLDEN, "tie_walks.npz"))
+    cases = {}
+    for key in z.files:
+        case, rest = key.split("/", 1)
+        cases.setdefault(case, {})[rest] = z[key]
+    return cases
+
+
+@pytest.fixture(scope="session")
 def ref_module():
     from oracle import oracle as O
     return O.load_reference_module()

@@ -23,8 +23,15 @@ has the reference checkout and oracle/_ref built; not needed at test time).
 4. ``slice_brute.npz``: Slice.makeSlice and BruteProjection.makeProjection
    (sum, max, min) of the reference module on a seeded uniform cloud with two
    fields, and a slice of its periodic counterpart.
+5. ``tie_walks.npz``: exact-tie geometry, where the answer depends on the
+   order in which the reference's tree meets equidistant generators:
+   segment lists of lattice clouds (the degenerate rays of the reference's
+   tests/test_degenerate.py, axis rays at face/edge offsets, rays between
+   half- and quarter-grid points, face diagonals, a float32-quantised
+   lattice), queryTree(q, k) on the half and quarter grids, and Slice /
+   BruteProjection samples on lattice faces and vertices.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference [galaxy|small|periodic|slice ...]]
+Usage:  python tests/golden/make_golden.py [/path/to/reference [galaxy|small|periodic|slice|ties ...]]
 """
 from __future__ import annotations
 
@@ -285,13 +292,146 @@ def slice_brute(mod):
     print("slice_brute.npz written")
 
 
+# the five degenerate rays of the reference's tests/test_degenerate.py on the
+# 5x5x5 lattice
+DEGENERATE_RAYS = [
+    ([-0.1] * 3, [4.1] * 3),
+    ([0.5, 0.2, -0.1], [0.5, 0.2, 4.1]),
+    ([0.5, 0.5, -0.1], [0.5, 0.5, 4.1]),
+    ([0.1] * 3, [0.9] * 3),
+    ([0.50001, 0.50001, -0.1], [0.50001, 0.50001, 4.1]),
+]
+
+
+def _tie_rays(rng, n):
+    """Rays on a 6x6x6 lattice whose walks meet exact distance ties: rays
+    along the axes at face, edge and interior offsets; rays between random
+    points of the half-integer grid (both ends on cell faces, edges or
+    vertices); rays between quarter-grid points; face diagonals."""
+    st, en = [], []
+    offs = [0.5, 1.0, 1.5, 2.25, 3.0]
+    for ax in range(3):
+        o = [d for d in range(3) if d != ax]
+        for a in offs:
+            for b in offs:
+                p = np.zeros(3)
+                q = np.zeros(3)
+                p[o[0]], p[o[1]] = a, b
+                q[o[0]], q[o[1]] = a, b
+                p[ax], q[ax] = -0.5, n - 0.5
+                st.append(p)
+                en.append(q)
+    half = np.arange(-0.5, n, 0.5)
+    for _ in range(100):
+        p, q = rng.choice(half, 3), rng.choice(half, 3)
+        if np.array_equal(p, q):
+            q[0] += 0.5
+        st.append(p)
+        en.append(q)
+    quarter = np.arange(-0.25, n - 0.5, 0.25)
+    for _ in range(60):
+        p, q = rng.choice(quarter, 3), rng.choice(quarter, 3)
+        if np.array_equal(p, q):
+            q[1] += 0.25
+        st.append(p)
+        en.append(q)
+    for _ in range(20):
+        ax = rng.integers(3)
+        c = rng.choice(half)
+        p = rng.uniform(-0.4, n - 0.6, 3)
+        p[ax] = c
+        q = p.copy()
+        o = [d for d in range(3) if d != ax]
+        p[o[0]], p[o[1]] = -0.5, -0.5
+        q[o[0]], q[o[1]] = n - 0.5, n - 0.5
+        st.append(p)
+        en.append(q)
+    return np.array(st), np.array(en)
+
+
+def tie_walks(mod):
+    """Exact-tie geometry through the reference module: segment lists of
+    lattice clouds (the degenerate rays of the reference's tests, axis rays,
+    half- and quarter-grid rays, face diagonals, a float32-quantised
+    lattice), the reference's k-NN order of exactly tied generators, and
+    Slice / BruteProjection samples on lattice faces and vertices."""
+    rng = np.random.default_rng(20241111)
+    blob = {}
+    cases = {}
+    pos, bb = lattice(5)
+    cases["lat5"] = (pos, bb, np.array([r[0] for r in DEGENERATE_RAYS + LATTICE_RAYS], float),
+                     np.array([r[1] for r in DEGENERATE_RAYS + LATTICE_RAYS], float))
+    pos, bb = lattice(6)
+    st, en = _tie_rays(rng, 6)
+    cases["lat6"] = (pos, bb, st, en)
+    pos, bb = lattice(8)
+    off = np.array([500.0, 500.0, 500.1])
+    p32 = (pos + off).astype(np.float32)
+    p32 -= off.astype(np.float32)
+    half = np.arange(-0.5, 8, 0.5)
+    st = np.array([rng.choice(half, 3) for _ in range(40)])
+    en = np.array([rng.choice(half, 3) for _ in range(40)])
+    en[np.all(st == en, axis=1), 0] += 0.5
+    cases["lat8_f32"] = (p32.astype(np.float64), bb, st, en)
+    for name, (pos, bb, st, en) in cases.items():
+        f = 1.0 + 0.001 * np.arange(len(pos))   # distinct per cell
+        keep = []
+        for i in range(len(st)):   # rays the reference walks without error
+            try:
+                O.reference_project(mod, pos, f, bb, st[i:i + 1], en[i:i + 1],
+                                    vol=np.ones(len(pos)))
+                keep.append(i)
+            except RuntimeError as e:
+                print(name, "ray", i, "skipped:", e)
+        st, en = st[keep], en[keep]
+        out, segs, oid = O.reference_project(mod, pos, f, bb, st, en, vol=np.ones(len(pos)),
+                                             detailed=True)
+        cid, se, sx, so = segs
+        blob.update({f"{name}/pos": pos, f"{name}/fields": f, f"{name}/bb": np.asarray(bb, float),
+                     f"{name}/vol": np.ones(len(pos)), f"{name}/starts": st, f"{name}/ends": en,
+                     f"{name}/out": np.asarray(out).reshape(len(st), -1),
+                     f"{name}/cell_ids": np.asarray(cid, np.int64),
+                     f"{name}/s_enter": np.asarray(se), f"{name}/s_exit": np.asarray(sx),
+                     f"{name}/offsets": np.asarray(so, np.int64),
+                     f"{name}/orig_ids": np.asarray(oid, np.int64)})
+        print(name, len(st), "rays,", len(cid), "segments")
+    # k-NN order of tied generators (queries on the half and quarter grids)
+    pos, bb = lattice(6)
+    pc = O.reference_cloud(mod, pos, np.ones(len(pos)), bb, vol=np.ones(len(pos)))
+    q = np.vstack([np.array([rng.choice(np.arange(-0.5, 6, 0.5), 3) for _ in range(200)]),
+                   np.array([rng.choice(np.arange(-0.25, 5.5, 0.25), 3) for _ in range(200)])])
+    blob["knn/q"] = q
+    for k in (1, 3, 8, 27):
+        ids = np.zeros((len(q), k), np.int64)
+        r2 = np.zeros((len(q), k))
+        for i, qq in enumerate(q):
+            a, b = pc.queryTree(qq, k)
+            ids[i], r2[i] = a, b
+        blob[f"knn/k{k}_ids"] = ids
+        blob[f"knn/k{k}_r2"] = r2
+    # Slice and BruteProjection sampling lattice faces, edges and vertices
+    f = np.column_stack([1.0 + np.arange(len(pos)), np.arange(len(pos))[::-1] * 0.5])
+    pc = O.reference_cloud(mod, pos, f, bb, vol=np.ones(len(pos)))
+    blob["sample/fields"] = f
+    for i, depth in enumerate((2.5, 2.0)):
+        sl = mod.Slice([13, 13], [-0.5, 5.5, -0.5, 5.5], depth)
+        sl.makeSlice(pc)
+        blob[f"sample/slice{i}"] = np.asarray(sl.returnSlice()).reshape(169, -1)
+    for mode in ("Sum", "Max", "Min"):
+        bp = mod.BruteProjection([13, 13, 13], [-0.5, 5.5, -0.5, 5.5, -0.5, 5.5])
+        bp.makeProjection(pc, getattr(mod.ReductionMode, mode))
+        blob[f"sample/brute_{mode.lower()}"] = np.asarray(bp.returnProjection()).reshape(169, -1)
+    np.savez_compressed(os.path.join(HERE, "tie_walks.npz"), **blob)
+    print("tie_walks.npz written")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     mod = O.load_reference_module()
     if mod is None:
         raise SystemExit("oracle/_ref/Cvortrace not built: run oracle/build_ref.sh first")
     warnings.simplefilter("ignore")
-    which = sys.argv[2:] or ["galaxy", "small", "periodic", "slice"]
+    which = sys.argv[2:] or ["galaxy", "small", "periodic", "slice", "ties"]
     if "galaxy" in which:
         galaxy(ref_root, mod)
     if "small" in which:
@@ -300,6 +440,8 @@ def main():
         periodic_walks(mod)
     if "slice" in which:
         slice_brute(mod)
+    if "ties" in which:
+        tie_walks(mod)
 
 
 if __name__ == "__main__":

@@ -2,9 +2,9 @@
 
 Bar: bit-exact cell ids, s values and integrals for integer/index work and
 the FP64 walk; volume rendering within 1e-12 relative (CUDA's exp vs
-glibc's).  Exact-tie geometry (lattices) is checked through the reference's
-invariants (integral = ray length, sum ds = length) because the device tree
-breaks exact k-NN ties in its own order."""
+glibc's).  Exact-tie geometry (lattices) is also checked through the
+reference's invariants (integral = ray length, sum ds = length) here; its
+segment lists are compared bit for bit in test_gpu_ties.py."""
 import warnings
 
 import numpy as np
@@ -69,7 +69,8 @@ def test_knn_lattice_distances():
     for k in (1, 3, 8):
         ids, r2 = pc._cloud.knn(q, k)
         oids, or2 = ot.knn(q, k)
-        np.testing.assert_array_equal(r2, or2)   # tie order may differ, distances may not
+        np.testing.assert_array_equal(r2, or2)
+        np.testing.assert_array_equal(ids, oids)   # tied points in nanoflann's order
 
 
 # ------------------------------------------------------- reference fixtures

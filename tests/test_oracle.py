@@ -42,6 +42,31 @@ def test_reference_fixtures_bit_exact(small_walks, case):
         np.testing.assert_array_equal(out, c[f"{mode}/out"])
 
 
+@pytest.mark.parametrize("case", ["lat5", "lat6", "lat8_f32"])
+def test_tie_fixtures_bit_exact(tie_walks, case):
+    # exact-tie geometry: the walk's 1-NN answers depend on nanoflann's order
+    c = tie_walks[case]
+    lp, t = oracle_for(c["pos"], c["fields"], c["bb"], c["vol"])
+    np.testing.assert_array_equal(lp["orig_ids"], c["orig_ids"])
+    out, (cid, se, sx, off) = t.project(c["starts"], c["ends"], "integrate", segments=True)
+    np.testing.assert_array_equal(off, c["offsets"])
+    np.testing.assert_array_equal(cid, c["cell_ids"])
+    np.testing.assert_array_equal(se, c["s_enter"])
+    np.testing.assert_array_equal(sx, c["s_exit"])
+    np.testing.assert_array_equal(out, c["out"])
+
+
+@pytest.mark.parametrize("k", [1, 3, 8, 27])
+def test_tie_knn_order(tie_walks, k):
+    from tests.conftest import make_cubic_lattice
+    pos, f, vol, bb = make_cubic_lattice(6)
+    lp, t = oracle_for(pos, f, bb, vol)
+    c = tie_walks["knn"]
+    ids, r2 = t.knn(c["q"], k)
+    np.testing.assert_array_equal(r2, c[f"k{k}_r2"])
+    np.testing.assert_array_equal(lp["orig_ids"][ids], c[f"k{k}_ids"])
+
+
 def test_split_point_known_answers():
     # tests/test_cpp.cpp:19-41 of the reference
     assert O.split_point_distance([0, 0, 0], [0, 0, 1], [0, 0, 0], [0, 0, 1]) == pytest.approx(0.5)

@@ -34,6 +34,7 @@ PARAM_LEAF_SIZE = 6
 PARAM_LOCAL_STACK = 7
 PARAM_CACHE = 8
 PARAM_ADJOINT_KERNEL = 9
+PARAM_DETAILED_KERNEL = 10
 
 # every symbol the header declares (checked by the tests)
 EXPORTS = (
@@ -48,6 +49,7 @@ EXPORTS = (
     "vt_tape_adjoint_device", "vt_slice", "vt_brute_projection", "vt_cloud_autotune",
     "vt_graph_create", "vt_graph_launch", "vt_graph_finish", "vt_graph_destroy",
     "vt_cloud_tree_save", "vt_cloud_tree_load", "vt_grid_rays_device", "vt_project_grid",
+    "vt_cloud_build_tie_tree",
 )
 
 
@@ -56,7 +58,9 @@ class CloudInfo(C.Structure):
                 ("subbox", C.c_double * 6), ("valid_rgba", C.c_int32),
                 ("tree_built", C.c_int32), ("periodic", C.c_int32), ("tree_depth", C.c_int32),
                 ("tree_leaves", C.c_uint64), ("tree_build_ms", C.c_double),
-                ("device_bytes", C.c_uint64)]
+                ("device_bytes", C.c_uint64), ("tie_tree_nodes", C.c_uint64),
+                ("tie_tree_depth", C.c_int32), ("reserved", C.c_int32),
+                ("tie_tree_build_ms", C.c_double)]
 
 
 class TuneResult(C.Structure):
@@ -75,7 +79,8 @@ class Stats(C.Structure):
                 ("fp64_resolves", C.c_uint64), ("slow_rays", C.c_uint64),
                 ("max_stack", C.c_uint64), ("walk_ms", C.c_double),
                 ("search_steps", C.c_uint64), ("fp64_checks", C.c_uint64),
-                ("cache_refreshes", C.c_uint64), ("cache_hits", C.c_uint64)]
+                ("cache_refreshes", C.c_uint64), ("cache_hits", C.c_uint64),
+                ("ties", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -120,6 +125,7 @@ def load(path: str | None = None):
         L.vt_cloud_create.argtypes = [dp, u64, dp, u64, u64, dp, dp, u64, C.c_int,
                                       C.POINTER(vp)]
         L.vt_cloud_build_tree.argtypes = [vp]
+        L.vt_cloud_build_tie_tree.argtypes = [vp]
         L.vt_cloud_set_param.argtypes = [vp, C.c_int, C.c_int64]
         L.vt_cloud_set_fields.argtypes = [vp, dp]
         L.vt_cloud_set_fields_device.argtypes = [vp, vp, vp]
@@ -161,7 +167,8 @@ def load(path: str | None = None):
         L.vt_project_device_tape.argtypes = [vp, vp, vp, vp, u64, C.c_int, C.c_int, vp, vp,
                                              C.POINTER(Stats)]
         L.vt_tape_adjoint_device.argtypes = [vp, vp, vp, vp, u64, C.c_int, vp, vp, vp, vp]
-        for name in ("vt_cloud_create", "vt_cloud_build_tree", "vt_cloud_set_param",
+        for name in ("vt_cloud_create", "vt_cloud_build_tree", "vt_cloud_build_tie_tree",
+                     "vt_cloud_set_param",
                      "vt_cloud_set_fields", "vt_cloud_set_fields_device",
                      "vt_cloud_get_info", "vt_cloud_orig_ids", "vt_knn", "vt_project",
                      "vt_project_device", "vt_project_device_noalloc", "vt_project_detailed",

@@ -275,6 +275,7 @@ int vt_cloud_build_tree(vt_cloud* cl) {
   if (vt::verbose()) std::cout << "Building tree...\n";
   auto t0 = std::chrono::high_resolution_clock::now();
   cl->tree_built = false;
+  vt::drop_tie_tree(cl);
   int rc = vt::build_tree_device(cl);
   if (rc) return rc;
   auto t1 = std::chrono::high_resolution_clock::now();
@@ -309,6 +310,7 @@ int vt_cloud_tree_load(vt_cloud* cl, const void* buf, uint64_t size) {
   VT_CUDA(cudaSetDevice(cl->device));
   auto t0 = std::chrono::high_resolution_clock::now();
   cl->tree_built = false;
+  vt::drop_tie_tree(cl);
   int rc = vt::load_tree_blob(cl, buf, size);
   if (rc) return rc;
   auto t1 = std::chrono::high_resolution_clock::now();
@@ -354,6 +356,11 @@ int vt_cloud_set_param(vt_cloud* cl, int param, int64_t value) {
       if (value < VT_KERNEL_AUTO || value > VT_KERNEL_THREAD_FP32)
         return set_error(VT_ERR_INVALID, "unknown kernel");
       cl->adjoint_kernel = (int)value;
+      return VT_OK;
+    case VT_PARAM_DETAILED_KERNEL:
+      if (value < VT_KERNEL_AUTO || value > VT_KERNEL_THREAD_FP32)
+        return set_error(VT_ERR_INVALID, "unknown kernel");
+      cl->detailed_kernel = (int)value;
       return VT_OK;
     case VT_PARAM_LEAF_SIZE:
       if (value < 2 || value > 64) return set_error(VT_ERR_INVALID, "leaf size out of range [2, 64]");
@@ -401,7 +408,12 @@ int vt_cloud_get_info(const vt_cloud* cl, vt_cloud_info* info) {
   info->tree_build_ms = cl->build_ms;
   info->device_bytes = cl->pts_d.bytes() + cl->pts32_d.bytes() + cl->nodes_d.bytes() +
                        cl->nodes32_d.bytes() + cl->perm_d.bytes() + cl->fields_d.bytes() +
-                       cl->boxlo_d.bytes() + cl->boxhi_d.bytes();
+                       cl->boxlo_d.bytes() + cl->boxhi_d.bytes() + cl->tt_nodes_d.bytes() +
+                       cl->tt_pts_d.bytes() + cl->tt_tid_d.bytes();
+  info->tie_tree_nodes = cl->view.tt_nodes ? cl->tt_nodes_d.n : 0;
+  info->tie_tree_depth = cl->view.tt_nodes ? cl->tt_depth : 0;
+  info->reserved = 0;
+  info->tie_tree_build_ms = cl->tt_ms;
   return VT_OK;
 }
 
@@ -584,10 +596,10 @@ int vt_project_detailed(vt_cloud* cl, const double* starts, const double* ends, 
                           cudaMemcpyHostToDevice, st));
   int64_t* d_counts = cl->ws_counts.p;
   int64_t* d_off = cl->ws_counts.p + nrays;
-  // pass 1: reduction + segment counts
-  rc = project_device_locked(cl, cl->ws_starts.p, cl->ws_ends.p, nrays, mode,
-                             VT_KERNEL_PLAIN_FP64, cl->ws_out.p, st, nullptr, vt::kOutCount,
-                             d_counts);
+  // pass 1: reduction + segment counts; both passes run the same kernel
+  const int kernel = resolve_kernel(cl, cl->detailed_kernel, nrays);
+  rc = project_device_locked(cl, cl->ws_starts.p, cl->ws_ends.p, nrays, mode, kernel,
+                             cl->ws_out.p, st, nullptr, vt::kOutCount, d_counts);
   if (rc) return rc;
   if ((rc = vt::scan_offsets(cl, d_counts, d_off, (int64_t)nrays, st))) return rc;
   VT_CUDA(cudaMemcpyAsync(offsets, d_off, (nrays + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
@@ -610,7 +622,7 @@ int vt_project_detailed(vt_cloud* cl, const double* starts, const double* ends, 
   io.seg_cell = sg->cell.p;
   io.seg_enter = sg->s_enter.p;
   io.seg_exit = sg->s_exit.p;
-  rc = vt::run_walk(cl, io, vt::kOutFill, mode, VT_KERNEL_PLAIN_FP64, st, nullptr);
+  rc = vt::run_walk(cl, io, vt::kOutFill, mode, kernel, st, nullptr);
   if (rc) return rc;
   VT_CUDA(cudaStreamSynchronize(st));
   if (vt::verbose()) {
@@ -685,12 +697,22 @@ static int grid_sample(vt_cloud* cl, bool brute, int mode, const uint64_t* npix,
   const uint64_t nf = cl->nfields;
   int rc;
   if ((rc = cl->ws_out.reserve(n * nf))) return rc;
-  if ((rc = cl->ws_slow.reserve(1))) return rc;
+  if ((rc = cl->ws_slow.reserve(2))) return rc;
   cudaStream_t st = cl->stream;
-  VT_CUDA(cudaMemsetAsync(cl->ws_slow.p, 0xff, sizeof(unsigned long long), st));
-  if ((rc = vt::run_grid_sample(cl, brute, mode, npix, lo, step, depth, cl->ws_out.p,
-                                cl->ws_slow.p, st)))
-    return rc;
+  unsigned long long flags[2] = {~0ULL, 0ULL};
+  for (int pass = 0; pass < 2; ++pass) {
+    // a sample that met an exact tie without the reference-order tree sets
+    // flags[1]: build the tree and sample again
+    VT_CUDA(cudaMemcpyAsync(cl->ws_slow.p, flags, sizeof(flags), cudaMemcpyHostToDevice, st));
+    if ((rc = vt::run_grid_sample(cl, brute, mode, npix, lo, step, depth, cl->ws_out.p,
+                                  cl->ws_slow.p, st)))
+      return rc;
+    unsigned long long got[2];
+    VT_CUDA(cudaMemcpyAsync(got, cl->ws_slow.p, sizeof(got), cudaMemcpyDeviceToHost, st));
+    VT_CUDA(cudaStreamSynchronize(st));
+    if (!got[1] || pass == 1) break;
+    if ((rc = vt::build_tie_tree(cl, st))) return rc;
+  }
   unsigned long long bad = 0;
   VT_CUDA(cudaMemcpyAsync(&bad, cl->ws_slow.p, sizeof(bad), cudaMemcpyDeviceToHost, st));
   if (n * nf > 0)

@@ -374,7 +374,10 @@ static __device__ __noinline__ RareOut rare_case1a(const DevCloud& c, RayGeom g,
       sn = perp_perturb(g, S, dadd(x, ex), dadd(y, ey), dadd(z, ez), cur, nxt);
     }
   }
-  RareOut o{0.0, (sc < 0 || sn < 0) ? kErrPerturb : 0, sc, sn, S.nq};
+  const int rc = (sc == kTieUnresolved || sn == kTieUnresolved) ? kNeedTie
+                 : (sc < 0 || sn < 0)                             ? kErrPerturb
+                                                                  : 0;
+  RareOut o{0.0, rc, sc, sn, S.nq};
   return o;
 }
 
@@ -491,7 +494,7 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
       phase = 0;
     };
     auto fail = [&](int rc) {
-      if (rc == kNeedSlow) hand_over(io, ray, nseg_of());
+      if (rc == kNeedSlow || rc == kNeedTie) hand_over(io, ray, nseg_of());
       else report(io, ray, rc);
       max_sp = max(max_sp, (unsigned)st.maxsp);
       phase = 0;
@@ -583,6 +586,8 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
     // ---- apply
     if (qkind != 0 && r.id[0] < 0) {
       fail(kErrNonFiniteDist);  // squared distances overflowed
+    } else if (qkind == 1 && r.id[1] >= 0 && r.r2[1] == r.r2[0]) {
+      fail(kNeedTie);  // exactly tied nearest cells: resolved in k_slow
     } else if (qkind == 1 && phase == 1) {
       c0 = r.id[0];
       phase = 2;
@@ -663,8 +668,8 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
   warp_add(&io.stats->fp64_resolves, n_res);
   warp_max(&io.stats->max_stack, max_sp);
 #if VT_BATCHED_COUNTERS
-  warp_add(&io.stats->pad[0], n_visit);
-  warp_add(&io.stats->pad[1], n_ver);
+  warp_add(&io.stats->search_steps, n_visit);
+  warp_add(&io.stats->fp64_checks, n_ver);
 #endif
 }
 

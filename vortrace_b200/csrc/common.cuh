@@ -41,8 +41,27 @@ constexpr int kErrNonFiniteDist = 17;  // squared distances overflowed
 constexpr int kErrPeriodicBisect = 18;  // no second cell on a periodic same-cell ray
 // internal: the ray must be finished by the degenerate-geometry kernel
 constexpr int kNeedSlow = 99;
+// internal: a 1-NN query met an exact tie and the reference-order tree is
+// not available in this kernel (or not built yet); the ray is finished by
+// k_slow, after the tree is built if need be
+constexpr int kNeedTie = 98;
+// status: an exact tie could not be resolved in the reference's order
+constexpr int kErrTie = 19;
+// 1-NN result: exact tie at the nearest distance, not resolved
+constexpr int kTieUnresolved = -2;
 
 enum Mode { kSum = 0, kMax = 1, kMin = 2, kVolume = 3 };
+
+// One node of the reference-order tree (tietree.cu): nanoflann's Node
+// (include/nanoflann.hpp:755-768) with explicit child indices.  feat < 0: a
+// leaf holding index-array slots [a, b); else split dimension `feat`,
+// children a (values <= lo) and b (values >= hi).
+struct __align__(16) TieNode {
+  double lo, hi;
+  int32_t feat, a, b, pad;
+};
+// deepest reference-order tree the tie-resolving search supports
+constexpr int kTieMaxDepth = 96;
 
 struct DevCloud {
   const double4* __restrict__ pts;
@@ -66,6 +85,11 @@ struct DevCloud {
   // periodic domain (src/pointcloud.cpp:26-32): the subbox and its side lengths
   int periodic;
   double sub_lo[3], sub_hi[3], box[3];
+  // reference-order tree (tietree.cu); NULL until an exact tie needs it
+  const TieNode* __restrict__ tt_nodes;
+  const double4* __restrict__ tt_pts;
+  const int32_t* __restrict__ tt_tid;
+  double tt_lo[3], tt_hi[3];  // its root box (computeBoundingBox)
 };
 
 // ---- FP64 arithmetic with the reference's rounding (no FMA contraction) --
@@ -127,7 +151,12 @@ struct DevStats {
   unsigned long long slow_count;   // rays queued for the degenerate kernel
   unsigned long long next_ray;     // work-queue head of the batched kernel
   unsigned long long next_slow;    // work-queue head of the degenerate kernel
-  unsigned long long pad[6];
+  unsigned long long search_steps;     // nodes (groups) the searches expanded
+  unsigned long long fp64_checks;      // FP64 re-checks of FP32-passing points
+  unsigned long long cache_refreshes;  // neighbourhood-cache refills (k_warp)
+  unsigned long long cache_hits;       // split queries answered from the cache
+  unsigned long long ties;             // 1-NN queries that met an exact tie
+  unsigned long long tie_deferred;     // rays waiting for the reference-order tree
 };
 
 // Sum a small per-lane value over the active lanes, one atomic per warp.

@@ -106,6 +106,7 @@ struct vt_cloud {
   int local_stack = 1 << 30;  // capped to the compiled size in the kernels
   int cache_mode = 0;
   int adjoint_kernel = VT_KERNEL_AUTO;  // kernel of the re-walk adjoint
+  int detailed_kernel = VT_KERNEL_AUTO;  // kernel of the detailed projection
   int tuned_kernel = VT_KERNEL_AUTO;    // vt_cloud_autotune's choice for AUTO
   uint64_t tuned_min_rays = 0;          // ... for batches at least this large
   // device tree (tree order)
@@ -116,6 +117,12 @@ struct vt_cloud {
   vt::DevBuf<int32_t> perm_d;
   vt::DevBuf<double> fields_d;
   vt::DevBuf<float4> boxlo_d, boxhi_d;
+  // reference-order tree (tietree.cu), built when an exact tie needs it
+  vt::DevBuf<vt::TieNode> tt_nodes_d;
+  vt::DevBuf<double4> tt_pts_d;
+  vt::DevBuf<int32_t> tt_tid_d;
+  int tt_depth = 0;
+  double tt_ms = 0.0;
   vt::DevCloud view{};
   double build_ms = 0.0;
   double cross_per_ray = 0.0;  // crossings per ray of the last walk (tape sizing)
@@ -150,6 +157,10 @@ struct vt_tape {
 
 namespace vt {
 int build_tree_device(vt_cloud* cl);
+// reference-order tree for exact ties (tietree.cu): build (no-op when built)
+// and free (the device tree was rebuilt or reloaded)
+int build_tie_tree(vt_cloud* cl, cudaStream_t st);
+void drop_tie_tree(vt_cloud* cl);
 // saved trees (tree_build.cu)
 uint64_t tree_blob_size(const vt_cloud* cl);
 int save_tree_blob(vt_cloud* cl, void* buf);

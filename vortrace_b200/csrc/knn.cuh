@@ -184,6 +184,88 @@ __device__ __noinline__ void knn_exact64(const DevCloud& c, double qx, double qy
   nvisit += visits;
 }
 
+// k-NN on the reference-order tree (tietree.cu) with nanoflann's traversal
+// state for state (include/nanoflann.hpp:1221-1241 findNeighbors,
+// 1005-1021 computeInitialDistances, 1346-1408 searchLevel): per-dimension
+// offsets dists[] updated as mindistsq + cut_dist - dists[idx] and restored
+// on the way back, the far child visited when its bound is <= the current
+// worst distance, a leaf's points tested against the worst distance read
+// on entering the leaf.  The recursion runs on an explicit frame stack
+// (state 0: descend into the nearer child; 1: decide the farther one;
+// 2: restore dists[idx]).  Results are device-tree indices.  Returns false
+// when the tree is deeper than the stack (refused when the tree is built).
+template <class List>
+__device__ __noinline__ bool knn_tieorder(const DevCloud& c, double qx, double qy, double qz,
+                                          List& res) {
+  const double q[3] = {qx, qy, qz};
+  double dists[3] = {0.0, 0.0, 0.0};
+  double distsq = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (q[i] < c.tt_lo[i]) {
+      dists[i] = dmul(dsub(q[i], c.tt_lo[i]), dsub(q[i], c.tt_lo[i]));
+      distsq = dadd(distsq, dists[i]);
+    }
+    if (q[i] > c.tt_hi[i]) {
+      dists[i] = dmul(dsub(q[i], c.tt_hi[i]), dsub(q[i], c.tt_hi[i]));
+      distsq = dadd(distsq, dists[i]);
+    }
+  }
+  int f_node[kTieMaxDepth];
+  int f_state[kTieMaxDepth];
+  double f_md[kTieMaxDepth], f_dst[kTieMaxDepth];
+  int sp = 0;
+  f_node[0] = 0;
+  f_state[0] = 0;
+  f_md[0] = distsq;
+  while (sp >= 0) {
+    const TieNode nd = c.tt_nodes[f_node[sp]];
+    if (nd.feat < 0) {
+      const double worst = res.worst();
+      for (int i = nd.a; i < nd.b; ++i) {
+        const double d = metric(qx, qy, qz, c.tt_pts[i]);
+        if (d < worst) res.insert(d, c.tt_tid[i]);
+      }
+      --sp;
+      continue;
+    }
+    const int idx = nd.feat;
+    const double val = q[idx];
+    const double diff1 = dsub(val, nd.lo);
+    const double diff2 = dsub(val, nd.hi);
+    const bool left_first = dadd(diff1, diff2) < 0;
+    if (f_state[sp] == 0) {
+      f_state[sp] = 1;
+      if (sp + 1 >= kTieMaxDepth) return false;
+      f_node[sp + 1] = left_first ? nd.a : nd.b;
+      f_state[sp + 1] = 0;
+      f_md[sp + 1] = f_md[sp];
+      ++sp;
+      continue;
+    }
+    if (f_state[sp] == 1) {
+      const double cut = left_first ? dmul(dsub(val, nd.hi), dsub(val, nd.hi))
+                                    : dmul(dsub(val, nd.lo), dsub(val, nd.lo));
+      const double dst = dists[idx];
+      const double md = dsub(dadd(f_md[sp], cut), dst);
+      dists[idx] = cut;
+      f_dst[sp] = dst;
+      f_state[sp] = 2;
+      if (md <= res.worst()) {
+        if (sp + 1 >= kTieMaxDepth) return false;
+        f_node[sp + 1] = left_first ? nd.b : nd.a;
+        f_state[sp + 1] = 0;
+        f_md[sp + 1] = md;
+        ++sp;
+        continue;
+      }
+    }
+    dists[idx] = f_dst[sp];
+    --sp;
+  }
+  return true;
+}
+
 // PointCloud::minDistSqToBox (src/pointcloud.cpp:283-297)
 __device__ __forceinline__ double min_dist_sq_to_box(const DevCloud& c, double x, double y,
                                                      double z) {
@@ -210,7 +292,7 @@ __device__ __forceinline__ double min_dist_sq_to_box(const DevCloud& c, double x
 // its smallest distance, sorted ascending, truncated to k.  (Equal
 // distances keep their merge order here; the reference's std::sort leaves
 // their order unspecified.)  `L` is KnnList<K> or KnnBig<KMAX>.
-template <int KMAX, class L>
+template <int KMAX, bool TT, class L>
 __device__ __noinline__ void knn_periodic_merge64(const DevCloud& c, double qx, double qy,
                                                   double qz, L& res, unsigned& nvisit) {
   const int k = res.capacity();
@@ -233,7 +315,8 @@ __device__ __noinline__ void knn_periodic_merge64(const DevCloud& c, double qx, 
         if (minD2 > dadd(worst, kTol)) continue;
         L img;
         img.clear(k);
-        knn_exact64(c, sx, sy, sz, __longlong_as_double(0x7ff0000000000000ULL), img, nvisit);
+        if (TT) knn_tieorder(c, sx, sy, sz, img);
+        else knn_exact64(c, sx, sy, sz, __longlong_as_double(0x7ff0000000000000ULL), img, nvisit);
         const int ni = img.count();
         for (int i = 0; i < ni; i++) {
           bool found = false;
@@ -276,24 +359,93 @@ __device__ __noinline__ void knn_periodic_merge64(const DevCloud& c, double qx, 
 // The k-NN of the reference's queryTreeK: exact FP64 search, then, in code
 // compiled with PER and on a periodic cloud, the periodic merge.  Kernels
 // that never serve periodic clouds compile without it (PER = false), which
-// keeps the merge out of their register allocation.
-template <int KMAX, bool PER, class L>
+// keeps the merge out of their register allocation.  TT: every search runs
+// on the reference-order tree (the caller checks that it is built), so
+// exactly tied points come in the reference's order.
+template <int KMAX, bool PER, class L, bool TT = false>
 __device__ __forceinline__ void knn_query64(const DevCloud& c, double qx, double qy, double qz,
                                             L& res, unsigned& nvisit) {
-  knn_exact64(c, qx, qy, qz, __longlong_as_double(0x7ff0000000000000ULL), res, nvisit);
+  if (TT) knn_tieorder(c, qx, qy, qz, res);
+  else knn_exact64(c, qx, qy, qz, __longlong_as_double(0x7ff0000000000000ULL), res, nvisit);
   if constexpr (PER) {
-    if (c.periodic && res.count() > 0) knn_periodic_merge64<KMAX>(c, qx, qy, qz, res, nvisit);
+    if (c.periodic && res.count() > 0) knn_periodic_merge64<KMAX, TT>(c, qx, qy, qz, res, nvisit);
   }
 }
 
-// Nearest neighbour (tree index) of q.
-template <bool PER = false>
-__device__ __forceinline__ int nn1_exact64(const DevCloud& c, double qx, double qy, double qz,
-                                           unsigned& nvisit) {
-  KnnList<1> r;
+// One search's nearest neighbour (tree index) and whether another point has
+// exactly the same distance (then the reference's answer depends on its
+// traversal order).  On the reference-order tree (TT) the answer is the
+// reference's and `tie` is not set.
+template <bool TT>
+__device__ __forceinline__ void nn1_search(const DevCloud& c, double x, double y, double z,
+                                           int& id, double& d, bool& tie, unsigned& nvisit) {
+  if (TT) {
+    KnnList<1> r;
+    r.clear();
+    knn_tieorder(c, x, y, z, r);
+    id = r.id[0];
+    d = r.r2[0];
+    return;
+  }
+  KnnList<2> r;
   r.clear();
-  knn_query64<1, PER>(c, qx, qy, qz, r, nvisit);
-  return r.id[0];
+  knn_exact64(c, x, y, z, __longlong_as_double(0x7ff0000000000000ULL), r, nvisit);
+  id = r.id[0];
+  d = r.r2[0];
+  tie = tie || (r.id[1] >= 0 && r.r2[1] == r.r2[0]);
+}
+
+// PointCloud::queryTree (src/pointcloud.cpp:300-306) with the periodic
+// 27-image merge (:313-367) at k = 1: an image's nearest replaces the
+// current one only when strictly closer (the reference's sort keeps the
+// earlier of equal entries) and the same particle keeps its smaller
+// distance.
+template <bool PER, bool TT>
+__device__ __forceinline__ int nn1_query(const DevCloud& c, double qx, double qy, double qz,
+                                         bool& tie, unsigned& nvisit) {
+  int id;
+  double d;
+  nn1_search<TT>(c, qx, qy, qz, id, d, tie, nvisit);
+  if (id < 0) return -1;
+  if constexpr (PER) {
+    if (c.periodic) {
+      for (int ix = -1; ix <= 1; ix++)
+        for (int iy = -1; iy <= 1; iy++)
+          for (int iz = -1; iz <= 1; iz++) {
+            if (ix == 0 && iy == 0 && iz == 0) continue;
+            const double sx = dadd(qx, dmul((double)ix, c.box[0]));
+            const double sy = dadd(qy, dmul((double)iy, c.box[1]));
+            const double sz = dadd(qz, dmul((double)iz, c.box[2]));
+            if (min_dist_sq_to_box(c, sx, sy, sz) > dadd(d, kTol)) continue;
+            int iid;
+            double idd;
+            nn1_search<TT>(c, sx, sy, sz, iid, idd, tie, nvisit);
+            if (iid < 0) continue;
+            if (iid == id) d = fmin(d, idd);
+            else if (idd < d) {
+              id = iid;
+              d = idd;
+            }
+          }
+    }
+  }
+  return id;
+}
+
+// Nearest neighbour (tree index) of q, the reference's answer: -1 when no
+// distance is finite; when the nearest distance is exactly shared, the
+// query is repeated on the reference-order tree if TIES and the tree is
+// built, else kTieUnresolved.  `nties` counts queries that met a tie.
+template <bool PER = false, bool TIES = false>
+__device__ __forceinline__ int nn1_exact64(const DevCloud& c, double qx, double qy, double qz,
+                                           unsigned& nvisit, unsigned* nties = nullptr) {
+  bool tie = false;
+  const int id = nn1_query<PER, false>(c, qx, qy, qz, tie, nvisit);
+  if (!tie || id < 0) return id;
+  if (nties) ++*nties;
+  if (!TIES || !c.tt_nodes) return kTieUnresolved;
+  bool unused = false;
+  return nn1_query<PER, true>(c, qx, qy, qz, unused, nvisit);
 }
 
 }  // namespace vt

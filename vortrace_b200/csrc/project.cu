@@ -40,7 +40,7 @@ __global__ void k_diag(DevCloud c, WalkIO io, int64_t ray) {
     io.diag->code = kErrNonFinite;
     return;
   }
-  Search64T<true> S(c);  // serves periodic and non-periodic clouds
+  Search64T<true, true> S(c);  // serves periodic and non-periodic clouds
   NullSink ns;
   int rc = walk_ray(c, g, io.max_iter, S, st, ns, io.diag);
   if (rc == kNeedSlow) rc = kErrStack;
@@ -52,14 +52,25 @@ __global__ void k_diag(DevCloud c, WalkIO io, int64_t ray) {
 }
 
 // -------------------------------------------------------------- k_knn
+// PointCloud::queryTree(q, k).  TT = false: the device tree, searched for
+// k + 1 neighbours so that an exact tie inside the list or across its end
+// is seen (then *tie is set and the host repeats the queries with TT = true,
+// on the reference-order tree, which lists tied points in the reference's
+// order).
+template <bool TT>
 __global__ void k_knn(DevCloud c, const double* __restrict__ q, int64_t nq, int k, int64_t* ids,
-                      double* r2) {
+                      double* r2, unsigned* tie) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= nq) return;
-  KnnBig<128> r;
-  r.clear(k);
+  KnnBig<129> r;
+  r.clear(TT ? k : (int)min((int64_t)k + 1, c.n));
   unsigned v = 0;
-  knn_query64<128, true>(c, q[3 * i], q[3 * i + 1], q[3 * i + 2], r, v);
+  knn_query64<129, true, KnnBig<129>, TT>(c, q[3 * i], q[3 * i + 1], q[3 * i + 2], r, v);
+  if (!TT) {
+    bool t = false;
+    for (int j = 0; j + 1 < r.cnt && j < k; ++j) t = t || r.r2[j] == r.r2[j + 1];
+    if (t) atomicOr(tie, 1u);
+  }
   for (int j = 0; j < k; ++j) {
     const bool ok = j < r.cnt;
     ids[i * k + j] = ok ? (int64_t)c.perm[r.id[j]] : -1;
@@ -127,8 +138,34 @@ static int finish_walk(vt_cloud* cl, WalkIO& io, const DevStats& hs, float ms, c
 // reference's error message.  `d_diag`: device scratch for the diagnosis of
 // a failing ray (NULL: allocated on demand).  `timed`: CUDA events around
 // the launches for vt_stats.walk_ms.
+// Rays deferred by k_slow for the reference-order tree (an exact tie at the
+// nearest distance of a 1-NN query, tietree.cu): build the tree if it is not
+// there (unless the caller cannot allocate: then an error naming
+// vt_cloud_build_tie_tree), run k_slow over the deferred rays and re-read
+// the counters into `hs`.
+static int complete_deferred(vt_cloud* cl, WalkIO& io, int out_kind, int mode, cudaStream_t st,
+                             bool may_alloc, DevStats& hs) {
+  if (hs.tie_deferred == 0) return VT_OK;
+  if (!cl->view.tt_nodes) {
+    if (!may_alloc)
+      return set_error(VT_ERR_RUNTIME,
+                       "an exact distance tie needs the reference-order tree, which this call "
+                       "does not allocate: build it first with vt_cloud_build_tie_tree");
+    const int rc = build_tie_tree(cl, st);
+    if (rc) return rc;
+  }
+  io.deferred = 1;
+  const int rc = launch_kind(cl, io, out_kind, mode, VT_KERNEL_AUTO, st);
+  io.deferred = 0;
+  if (rc) return rc;
+  VT_CUDA(cudaMemcpyAsync(&hs, io.stats, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  return VT_OK;
+}
+
 static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel,
-                       cudaStream_t st, vt_stats* stats, WalkDiag* d_diag, bool timed) {
+                       cudaStream_t st, vt_stats* stats, WalkDiag* d_diag, bool timed,
+                       bool may_alloc = true) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (timed) {
     VT_CUDA(cudaEventCreate(&e0));
@@ -153,6 +190,8 @@ static int run_walk_on(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int ker
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   }
+  const int rc2 = complete_deferred(cl, io, out_kind, mode, st, may_alloc, hs);
+  if (rc2) return rc2;
   return finish_walk(cl, io, hs, ms, st, stats, d_diag);
 }
 
@@ -169,10 +208,11 @@ static int finish_walk(vt_cloud* cl, WalkIO& io, const DevStats& hs, float ms, c
     stats->slow_rays = hs.slow_rays;
     stats->max_stack = hs.max_stack;
     stats->walk_ms = ms;
-    stats->search_steps = hs.pad[0];
-    stats->fp64_checks = hs.pad[1];
-    stats->cache_refreshes = hs.pad[2];
-    stats->cache_hits = hs.pad[3];
+    stats->search_steps = hs.search_steps;
+    stats->fp64_checks = hs.fp64_checks;
+    stats->cache_refreshes = hs.cache_refreshes;
+    stats->cache_hits = hs.cache_hits;
+    stats->ties = hs.ties;
   }
   if (hs.first_error != ~0ULL) {
     const int64_t ray = (int64_t)(hs.first_error >> 8);
@@ -224,6 +264,9 @@ static int finish_walk(vt_cloud* cl, WalkIO& io, const DevStats& hs, float ms, c
                                              std::to_string(ray) + ": coordinates too large");
       case kErrPeriodicBisect:
         msg = "Could not find intermediate cell by bisection along periodic ray";
+        break;
+      case kErrTie:
+        msg = "an exact distance tie could not be resolved in the reference's order";
         break;
       default: msg = "ray walk failed with code " + std::to_string(code); break;
     }
@@ -370,6 +413,7 @@ struct vt_graph {
   vt::DevBuf<double> stack_s;
   vt::DevBuf<uint8_t> order;
   vt::WalkIO io{};
+  int mode = 0;
   const double4* pts = nullptr;  // the cloud's buffers at capture time
   const double* fields = nullptr;
   ~vt_graph() {
@@ -400,6 +444,7 @@ int vt_graph_create(vt_cloud* cl, const double* d_starts, const double* d_ends, 
         (rc = g->stack_id.alloc((size_t)slow_threads * cl->stack_cap)) ||
         (rc = g->stack_s.alloc((size_t)slow_threads * cl->stack_cap)))
       return rc;
+    g->mode = mode;
     WalkIO& io = g->io;
     io.starts = d_starts;
     io.ends = d_ends;
@@ -467,6 +512,9 @@ int vt_graph_finish(vt_graph* g, void* stream, vt_stats* stats) {
   DevStats hs;
   VT_CUDA(cudaMemcpyAsync(&hs, g->io.stats, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
   VT_CUDA(cudaStreamSynchronize(st));
+  // rays deferred for the reference-order tree finish here, outside the graph
+  const int rc = complete_deferred(g->cl, g->io, kOutImage, g->mode, st, true, hs);
+  if (rc) return rc;
   return finish_walk(g->cl, g->io, hs, 0.f, st, stats, nullptr);
 }
 
@@ -603,7 +651,11 @@ __global__ void k_slice(DevCloud c, uint64_t nx, uint64_t ny, double x0, double 
   const double qx = dadd(x0, dmul(dx, (double)i));
   const double qy = dadd(y0, dmul(dy, (double)j));
   unsigned v = 0;
-  const int cell = nn1_exact64<true>(c, qx, qy, depth, v);
+  const int cell = nn1_exact64<true, true>(c, qx, qy, depth, v);
+  if (cell == kTieUnresolved) {
+    atomicOr(&bad[1], 1ULL);
+    return;
+  }
   if (cell < 0) {
     atomicMin(bad, (unsigned long long)t);
     return;
@@ -631,7 +683,11 @@ __global__ void k_brute(DevCloud c, uint64_t nx, uint64_t ny, uint64_t nz, doubl
   for (uint64_t k = 0; k < nz; k++) {
     const double qz = dadd(z0, dmul(dz, (double)k));
     unsigned v = 0;
-    const int cell = nn1_exact64<true>(c, qx, qy, qz, v);
+    const int cell = nn1_exact64<true, true>(c, qx, qy, qz, v);
+    if (cell == kTieUnresolved) {
+      atomicOr(&bad[1], 1ULL);
+      return;
+    }
     if (cell < 0) {
       atomicMin(bad, (unsigned long long)t);
       return;
@@ -647,8 +703,10 @@ __global__ void k_brute(DevCloud c, uint64_t nx, uint64_t ny, uint64_t nz, doubl
     for (int f = 0; f < nf; f++) row[f] = dmul(row[f], dz);
 }
 
-// Launch one of the two; `bad` (device, one slot) receives the first pixel
-// whose query had no finite distance (UINT64_MAX when none).
+// Launch one of the two; `bad` (device, two slots) receives the first pixel
+// whose query had no finite distance (UINT64_MAX when none) and, in bad[1],
+// 1 when a sample met an exact tie while the reference-order tree was not
+// built (the host then builds it and samples again).
 int run_grid_sample(vt_cloud* cl, bool brute, int mode, const uint64_t* npix, const double* lo,
                     const double* step, double depth, double* d_out, unsigned long long* d_bad,
                     cudaStream_t st) {
@@ -674,10 +732,25 @@ int run_grid_sample(vt_cloud* cl, bool brute, int mode, const uint64_t* npix, co
   return VT_OK;
 }
 
+// k-NN of nq device queries; exact ties in the reference's order (a second
+// pass on the reference-order tree when the first saw one).  Synchronises.
 int run_knn(vt_cloud* cl, const double* d_q, int64_t nq, int k, int64_t* d_ids, double* d_r2,
             cudaStream_t st) {
   const int B = 128;
-  if (nq > 0) k_knn<<<(unsigned)((nq + B - 1) / B), B, 0, st>>>(cl->view, d_q, nq, k, d_ids, d_r2);
+  if (nq <= 0) return VT_OK;
+  if (cl->ws_stats.reserve(1)) return VT_ERR_NOMEM;
+  unsigned* d_tie = reinterpret_cast<unsigned*>(cl->ws_stats.p);
+  VT_CUDA(cudaMemsetAsync(d_tie, 0, sizeof(unsigned), st));
+  const unsigned blocks = (unsigned)((nq + B - 1) / B);
+  k_knn<false><<<blocks, B, 0, st>>>(cl->view, d_q, nq, k, d_ids, d_r2, d_tie);
+  VT_CUDA(cudaGetLastError());
+  unsigned tie = 0;
+  VT_CUDA(cudaMemcpyAsync(&tie, d_tie, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  if (!tie) return VT_OK;
+  const int rc = build_tie_tree(cl, st);
+  if (rc) return rc;
+  k_knn<true><<<blocks, B, 0, st>>>(cl->view, d_q, nq, k, d_ids, d_r2, d_tie);
   VT_CUDA(cudaGetLastError());
   return VT_OK;
 }
@@ -779,7 +852,7 @@ extern "C" int vt_project_device_noalloc(vt_cloud* cl, const double* d_starts,
     // counters and the first-error slot are cleared by run_walk_on; the
     // queue and stacks need no clearing (written before they are read)
     return run_walk_on(cl, io, kOutImage, mode, VT_KERNEL_BATCHED, st, nullptr,
-                       reinterpret_cast<WalkDiag*>(base + kNoAllocOffDiag), false);
+                       reinterpret_cast<WalkDiag*>(base + kNoAllocOffDiag), false, false);
   } catch (const std::exception& e) {
     return set_error(VT_ERR_RUNTIME, e.what());
   }

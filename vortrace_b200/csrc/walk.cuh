@@ -114,16 +114,19 @@ struct GlobalStack {
 // ------------------------------------------------------- exact FP64 search
 // Full-featured search policy (plain kernel and degenerate-geometry kernel);
 // PER: also serves periodic clouds (periodic k-NN merge, minimum-image split
-// points, same-cell bisection).
-template <bool PER>
+// points, same-cell bisection).  TIES: a 1-NN query whose nearest distance
+// is exactly shared is answered on the reference-order tree when it is
+// built; otherwise (and always without TIES) nn1 returns kTieUnresolved and
+// the walk stops with kNeedTie.
+template <bool PER, bool TIES = false>
 struct Search64T {
   const DevCloud& c;
-  unsigned nq = 0, nvisit = 0;
+  unsigned nq = 0, nvisit = 0, nties = 0;
   static constexpr bool kPeriodic = PER;
   __device__ explicit Search64T(const DevCloud& cc) : c(cc) {}
   __device__ __forceinline__ int nn1(double x, double y, double z) {
     ++nq;
-    return nn1_exact64<PER>(c, x, y, z, nvisit);
+    return nn1_exact64<PER, TIES>(c, x, y, z, nvisit, &nties);
   }
   // 3-NN at a split point between cells cid and nid
   __device__ __forceinline__ int knn3(double x, double y, double z, int cid, int nid,
@@ -180,6 +183,7 @@ __device__ int split_full(const DevCloud& c, const RayGeom& g, S& srch, int id1,
     double x, y, z;
     ray_point(g, mid, x, y, z);
     const int mc = srch.nn1(x, y, z);
+    if (mc == kTieUnresolved) return kNeedTie;
     if (mc < 0) return kErrNonFiniteDist;
     if (mc != id1 && mc != id2) {
       s_out = mid;
@@ -195,7 +199,8 @@ __device__ int split_full(const DevCloud& c, const RayGeom& g, S& srch, int id1,
   return kErrBinSearch;
 }
 
-// Ray::perpPerturbToFindCell (src/ray.cpp:129-185); returns -1 on failure.
+// Ray::perpPerturbToFindCell (src/ray.cpp:129-185); returns -1 on failure,
+// kTieUnresolved when a query met a tie it could not resolve.
 template <class S>
 __device__ int perp_perturb(const RayGeom& g, S& srch, double px, double py, double pz, int ex1,
                             int ex2) {
@@ -230,6 +235,7 @@ __device__ int perp_perturb(const RayGeom& g, S& srch, double px, double py, dou
 #pragma unroll
           for (int j = 0; j < 3; j++) pt[j] = dadd(pos[j], dmul(kPerturbEps, cr[j]));
           const int cell = srch.nn1(pt[0], pt[1], pt[2]);
+          if (cell == kTieUnresolved) return kTieUnresolved;
           if (cell != ex1 && cell != ex2) return cell;
           cycle++;
         }
@@ -272,13 +278,16 @@ __device__ __noinline__ int expand_classify(const DevCloud& c, double x, double 
 }
 
 // Ray::walk (src/ray.cpp:187-430).  Emits segments in order to
-// `sink.seg(cell, s_enter, s_exit)`.  Returns 0, an error code, or kNeedSlow
-// (search policy with kDefer, or a stack without room).
+// `sink.seg(cell, s_enter, s_exit)`.  Returns 0, an error code, kNeedSlow
+// (search policy with kDefer, or a stack without room) or kNeedTie (a 1-NN
+// query met an exact tie the search policy cannot resolve; every segment
+// emitted before it is the reference's).
 template <class S, class Stack, class Sink>
 __device__ int walk_ray(const DevCloud& c, const RayGeom& g, int64_t max_iter, S& srch,
                         Stack& st, Sink& sink, WalkDiag* diag) {
   const int c0 = srch.nn1(g.s[0], g.s[1], g.s[2]);
   const int c1 = srch.nn1(g.e[0], g.e[1], g.e[2]);
+  if (c0 == kTieUnresolved || c1 == kTieUnresolved) return kNeedTie;
   if (c0 < 0 || c1 < 0) return kErrNonFiniteDist;  // squared distances overflowed
   int open_cell = c0;
   double entry_s = 0.0;
@@ -300,6 +309,7 @@ __device__ int walk_ray(const DevCloud& c, const RayGeom& g, int64_t max_iter, S
         double x, y, z;
         ray_point(g, mid_s, x, y, z);
         const int mc = srch.nn1(x, y, z);
+        if (mc == kTieUnresolved) return kNeedTie;
         if (mc < 0) return kErrNonFiniteDist;
         if (mc != c0) {
           st.push(mc, mid_s);
@@ -401,6 +411,7 @@ __device__ int walk_ray(const DevCloud& c, const RayGeom& g, int64_t max_iter, S
         const double ex = dmul(kPerturbEps, g.d[0]), ey = dmul(kPerturbEps, g.d[1]),
                      ez = dmul(kPerturbEps, g.d[2]);
         sc = perp_perturb(g, srch, dsub(x, ex), dsub(y, ey), dsub(z, ez), cur, nxt);
+        if (sc == kTieUnresolved) return kNeedTie;
         if (sc < 0) {
           if (diag) diag->code = kErrPerturb;
           return kErrPerturb;
@@ -411,6 +422,7 @@ __device__ int walk_ray(const DevCloud& c, const RayGeom& g, int64_t max_iter, S
         const double ex = dmul(kPerturbEps, g.d[0]), ey = dmul(kPerturbEps, g.d[1]),
                      ez = dmul(kPerturbEps, g.d[2]);
         sn = perp_perturb(g, srch, dadd(x, ex), dadd(y, ey), dadd(z, ez), cur, nxt);
+        if (sn == kTieUnresolved) return kNeedTie;
         if (sn < 0) {
           if (diag) diag->code = kErrPerturb;
           return kErrPerturb;

@@ -308,7 +308,7 @@ __device__ __forceinline__ int run_ray(const DevCloud& c, const WalkIO& io, int6
 }
 
 __device__ __forceinline__ void report(const WalkIO& io, int64_t ray, int rc) {
-  if (rc && rc != kNeedSlow)
+  if (rc && rc != kNeedSlow && rc != kNeedTie)
     atomicMin(&io.stats->first_error, ((unsigned long long)ray << 8) | (unsigned)rc);
 }
 
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(128) k_plain(DevCloud c, WalkIO io) {
   st.clear();
   unsigned nseg = 0;
   int rc = run_ray<MODE, NF, OUT>(c, io, ray, S, st, 0u, nseg);
-  if (rc == kNeedSlow) hand_over(io, ray, nseg);
+  if (rc == kNeedSlow || rc == kNeedTie) hand_over(io, ray, nseg);
   report(io, ray, rc);
   warp_add(&io.stats->rays, 1u);
   warp_add(&io.stats->crossings, rc == 0 ? nseg : 0u);
@@ -336,7 +336,20 @@ __global__ void __launch_bounds__(128) k_plain(DevCloud c, WalkIO io) {
   warp_max(&io.stats->max_stack, (unsigned)st.maxsp);
 }
 
+// hand-over queue entries: ray in bits 24-62, segments already emitted in
+// bits 0-23; bit 63 marks a ray deferred until the reference-order tree
+// exists
+constexpr unsigned long long kDeferredBit = 1ULL << 63;
+__device__ __forceinline__ int64_t queued_ray(unsigned long long e) {
+  return (int64_t)((e & ~kDeferredBit) >> 24);
+}
+
 // ------------------------------------------------------------- k_slow
+// Finishes the handed-over rays.  A ray whose 1-NN query meets an exact tie
+// while the reference-order tree is not built yet is deferred: its queue
+// entry is marked (with the segments emitted up to the tie, all of them the
+// reference's) and the host builds the tree and runs this kernel again with
+// io.deferred set, over the marked entries only.
 template <int MODE, int NF, int OUT, bool PER>
 __global__ void __launch_bounds__(128) k_slow(DevCloud c, WalkIO io) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -348,15 +361,23 @@ __global__ void __launch_bounds__(128) k_slow(DevCloud c, WalkIO io) {
   const unsigned long long total = io.stats->slow_count;
   for (unsigned long long q = tid; q < total; q += io.slow_threads) {
     const unsigned long long e = io.slow_q[q];
-    const int64_t ray = (int64_t)(e >> 24);
+    if (io.deferred && !(e & kDeferredBit)) continue;
+    const int64_t ray = queued_ray(e);
     const unsigned skip = (unsigned)(e & 0xffffffu);
-    Search64T<PER> S(c);
+    Search64T<PER, true> S(c);
     unsigned nseg = 0;
     int rc = run_ray<MODE, NF, OUT>(c, io, ray, S, st, skip, nseg);
     if (rc == kNeedSlow) rc = kErrStack;
-    report(io, ray, rc);
-    atomicAdd(&io.stats->slow_rays, 1ULL);
-    if (rc == 0) atomicAdd(&io.stats->crossings, (unsigned long long)nseg);
+    if (rc == kNeedTie && !io.deferred) {
+      io.slow_q[q] = kDeferredBit | ((unsigned long long)ray << 24) | (nseg & 0xffffffu);
+      atomicAdd(&io.stats->tie_deferred, 1ULL);
+    } else {
+      if (rc == kNeedTie) rc = kErrTie;
+      report(io, ray, rc);
+      if (rc == 0) atomicAdd(&io.stats->crossings, (unsigned long long)nseg);
+      if (S.nties) atomicAdd(&io.stats->ties, (unsigned long long)S.nties);
+    }
+    if (!io.deferred) atomicAdd(&io.stats->slow_rays, 1ULL);
     atomicAdd(&io.stats->queries, (unsigned long long)S.nq);
     atomicMax(&io.stats->max_stack, (unsigned long long)st.maxsp);
   }
@@ -378,7 +399,9 @@ int launch_walk_t(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) {
   const DevCloud& c = cl->view;
   if (io.nrays > 0) {
     const int B = 128;
-    if (cl->periodic) {
+    if (io.deferred) {
+      // second pass over the rays deferred for the reference-order tree
+    } else if (cl->periodic) {
       k_plain<MODE, NF, OUT, true><<<(unsigned)((io.nrays + B - 1) / B), B, 0, st>>>(c, io);
     } else if (kernel == VT_KERNEL_PLAIN_FP64) {
       k_plain<MODE, NF, OUT, false><<<(unsigned)((io.nrays + B - 1) / B), B, 0, st>>>(c, io);

@@ -64,6 +64,8 @@ struct WalkIO {
   unsigned long long* tape_count;  // kOutTape: entries appended (may exceed tape_cap)
   unsigned long long tape_cap;
   WalkDiag* diag;
+  int deferred;          // k_slow only, over the entries deferred for the
+                         // reference-order tree (which is now built)
 };
 
 int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaStream_t st,

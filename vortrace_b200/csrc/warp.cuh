@@ -739,9 +739,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
     // ---- end cells: leaf on the split-plane path, then a bounded search
     WarpQuery Q;
     Q.qe = qe;
+    // (2 nearest, so that an exact tie at the nearest distance is seen:
+    // such a ray is handed to k_slow, which answers it in the reference's
+    // order)
     auto nn_end = [&](double x, double y, double z) -> int {
       warp_query_setup(Q, c, x, y, z);
-      KnnList<1> r1;
+      KnnList<2> r1;
       r1.clear();
       const int64_t leaf = warp_descend_leaf(c, Q.q0, Q.q1, Q.q2);
       const int64_t a = (leaf * c.n) >> c.depth;
@@ -761,7 +764,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
       Q.cid = Q.nid = -1;
       Q.dc = Q.dn = 0.0;
       ++n_q;
-      if (!warp_knn<1>(c, lane, Q, leaf, r1, s_node, s_mind, n_ver, n_steps)) {
+      if (!warp_knn<2>(c, lane, Q, leaf, r1, s_node, s_mind, n_ver, n_steps)) {
         // search stack overflow: exact thread-level search by lane 0
         ++n_res;
         int id = -1;
@@ -769,12 +772,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
           unsigned v = 0;
           id = nn1_exact64(c, x, y, z, v);
         }
-        r1.id[0] = __shfl_sync(kFull, id, 0);
+        return __shfl_sync(kFull, id, 0);
       }
+      if (r1.id[0] >= 0 && r1.id[1] >= 0 && r1.r2[1] == r1.r2[0]) return kTieUnresolved;
       return r1.id[0];
     };
     const int c0 = nn_end(g.s[0], g.s[1], g.s[2]);
     const int c1 = nn_end(g.e[0], g.e[1], g.e[2]);
+    if (c0 == kTieUnresolved || c1 == kTieUnresolved) {
+      if (lane == 0) hand_over(io, ray, 0u);
+      continue;
+    }
     if (c0 < 0 || c1 < 0) {
       if (lane == 0) report(io, ray, kErrNonFiniteDist);
       continue;
@@ -975,7 +983,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
       }
       n_cross += nseg_now();
     } else if (lane == 0) {
-      if (rc == kNeedSlow) hand_over(io, ray, nseg_now());
+      if (rc == kNeedSlow || rc == kNeedTie) hand_over(io, ray, nseg_now());
       else report(io, ray, rc);
     }
     __syncwarp();
@@ -986,10 +994,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, VT_WARP_MINB) k_warp(DevC
     atomicAdd(&io.stats->queries, (unsigned long long)n_q);
     atomicAdd(&io.stats->fp64_resolves, (unsigned long long)n_res);
     atomicMax(&io.stats->max_stack, (unsigned long long)max_sp);
-    atomicAdd(&io.stats->pad[0], (unsigned long long)n_steps);
-    atomicAdd(&io.stats->pad[1], (unsigned long long)n_ver);
-    atomicAdd(&io.stats->pad[2], (unsigned long long)n_refresh);
-    atomicAdd(&io.stats->pad[3], (unsigned long long)n_hit);
+    atomicAdd(&io.stats->search_steps, (unsigned long long)n_steps);
+    atomicAdd(&io.stats->fp64_checks, (unsigned long long)n_ver);
+    atomicAdd(&io.stats->cache_refreshes, (unsigned long long)n_refresh);
+    atomicAdd(&io.stats->cache_hits, (unsigned long long)n_hit);
   }
 }
 

@@ -165,8 +165,9 @@ def _project(cloud: _Cloud, starts, ends, mode, kernel, nout):
     return out, st
 
 
-def _project_detailed(cloud: _Cloud, starts, ends, mode, nout):
+def _project_detailed(cloud: _Cloud, starts, ends, mode, nout, kernel="auto"):
     n = starts.shape[0]
+    cloud.set_param(L.PARAM_DETAILED_KERNEL, L.KERNELS[kernel])
     out = np.empty((n, nout), np.float64)
     offsets = np.empty(n + 1, np.int64)
     seg = C.c_void_p()
@@ -359,7 +360,8 @@ class ProjectionCloud:
         nout = self._nout(mode)
         if ps.shape[0] == 0:
             raise RuntimeError("Projection has not yet been made")
-        out, cid, se, sx, offsets = _project_detailed(self._cloud, ps, pe, mode, nout)
+        out, cid, se, sx, offsets = _project_detailed(self._cloud, ps, pe, mode, nout,
+                                                      self.kernel)
         values = _as_values(out, nout)
         cell_ids = self.orig_ids[cid]
         ds_vals = sx - se
