@@ -50,11 +50,11 @@ BX = {"clustered_2m": 3262.25, "uniform_100k": 2915.74, "volume_2m": 3273.36,
       "batched_1m": 3201.12, "nested_16m": 3320.48}
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per crossing of
-# the guarded-FP32 kernel, from one ncu capture of the 512x512 case of
-# clustered_2m (profiles/k_batched_fp32_clustered_2m_npix512.md: 4.35 GB for
-# 49,726,019 crossings); the full-size launch is taken to scale with its
+# the walk kernel, from one ncu capture of a smaller grid of the same cloud
+# (512x512 rays of clustered_2m: 4.35 GB for 49,726,019 crossings), keyed by
+# (workload, AUTO kernel); the full-size launch is taken to scale with its
 # crossings.
-DRAM_BYTES_PER_CROSSING = {"clustered_2m": 87.5}
+DRAM_BYTES_PER_CROSSING = {("clustered_2m", "thread_fp32"): 87.5}
 
 
 def dist_env():
@@ -218,28 +218,103 @@ def run_reference(args):
     return 0
 
 
-def run_ours(args):
+def oracle_sample_parity(w, pc, kernel, nsample=4096):
+    """Outside the timed region: the walk kernel's CSR segments of an evenly
+    spaced sample of the workload's rays against the oracle (the C
+    restatement of the reference, pinned to the reference module), and its
+    per-ray values against the oracle's."""
+    from oracle import oracle as O
+    n = w["starts"].shape[0]
+    idx = np.linspace(0, n - 1, min(nsample, n)).astype(np.int64)
+    S = np.ascontiguousarray(w["starts"][idx])
+    E = np.ascontiguousarray(w["ends"][idx])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        lp = O.load_points(w["pos"], w["fields"], w["boundbox"])
+    t = O.OracleTree(lp["pts"], lp["fields"], lp["valid_rgba"])
+    oout, (ocid, ose, osx, ooff) = t.project(S, E, w["reduction"], segments=True)
+    del t
+    old = pc.kernel
+    pc.kernel = kernel
+    try:
+        vals, cid, se, ds, off = pc.traced_projection(S, E, return_midpoint=False,
+                                                      reduction=w["reduction"], flatten=True)
+    finally:
+        pc.kernel = old
+    seg_ok = (np.array_equal(off, ooff) and np.array_equal(cid, lp["orig_ids"][ocid])
+              and np.array_equal(se, ose) and np.array_equal(ds, osx - ose))
+    v = np.asarray(vals).reshape(len(idx), -1)
+    o = oout.reshape(len(idx), -1)
+    rel = np.abs(v - o) / np.maximum(np.abs(o), 1e-300)
+    return {"sample_rays": int(len(idx)), "sample_crossings": int(ooff[-1]),
+            "segments_bit_identical_to_oracle": bool(seg_ok),
+            "values_bit_identical_to_oracle": bool(np.array_equal(v, o)),
+            "values_max_rel_err_vs_oracle": float(rel.max()) if rel.size else 0.0}, idx, o
+
+
+def counters_run(w, kernel, smem_levels, mode):
+    """One forward of the guarded-FP32 kernel through the library built
+    with the search counters (libvortrace_b200_counters.so), outside the
+    timed region: nodes visited, FP64 re-checks and the queries that needed
+    one."""
+    from vortrace_b200 import _lib as L
+    from vortrace_b200 import build as B
+    if not os.path.exists(B.LIB_COUNTERS):
+        return None
+    lib = L.load_variant(B.LIB_COUNTERS)
+    pos = np.ascontiguousarray(w["pos"], np.float64)
+    f = np.ascontiguousarray(w["fields"], np.float64)
+    nf = 1 if f.ndim == 1 else f.shape[1]
+    sb = np.ascontiguousarray(w["boundbox"], np.float64)
+    h = C.c_void_p()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        L.check(lib.vt_cloud_create(L.dptr(pos), pos.shape[0], L.dptr(f), pos.shape[0], nf,
+                                    L.dptr(sb), None, 0, 0, C.byref(h)), lib)
+    try:
+        L.check(lib.vt_cloud_build_tree(h), lib)
+        L.check(lib.vt_cloud_set_param(h, L.PARAM_SMEM_LEVELS, int(smem_levels)), lib)
+        S = np.ascontiguousarray(w["starts"])
+        E = np.ascontiguousarray(w["ends"])
+        n = S.shape[0]
+        nout = 3 if mode == L.REDUCE_VOLUME else nf
+        out = np.empty((n, nout))
+        st = L.Stats()
+        L.check(lib.vt_project(h, L.dptr(S), L.dptr(E), n, mode, kernel, L.dptr(out),
+                               C.byref(st)), lib)
+    finally:
+        lib.vt_cloud_destroy(h)
+    q32 = max(1, st.fp32_queries)
+    return {"kernel": "k_batched guarded-FP32 (library built with VT_BATCHED_COUNTERS=1)",
+            "queries": int(st.queries), "fp32_split_queries": int(st.fp32_queries),
+            "nodes_per_query": round(st.search_steps / max(1, st.queries), 3),
+            "fp64_rechecks_per_query": round(st.fp64_checks / q32, 4),
+            "queries_with_fp64_recheck_fraction": round(st.fp64_check_queries / q32, 6),
+            "fp64_full_resolves": int(st.fp64_resolves),
+            "fp64_full_resolve_fraction": round(st.fp64_resolves / max(1, st.queries), 8)}
+
+
+def measure(name, args, rank, world, dev, K, W, *, kp=None, wp=None, full=True,
+            npix=None):
+    """All legs of one workload.  K/W: timed and warm-up steps of the
+    headline legs; kp/wp: of the baseline legs (default max(2, K//2) / 1).
+    full: also the end-to-end leg through host buffers and the CPU leg."""
     import torch
-    import torch.distributed as dist
-    from datetime import timedelta
 
     import vortrace_b200 as vt
     from vortrace_b200 import _lib as L
 
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    L.load().vt_set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    dev = torch.device("cuda", local)
-    w = make_workload(args.config, rank, world, args.npix)
+    kp = kp if kp is not None else max(2, K // 2)
+    wp = wp if wp is not None else 1
+    w = make_workload(name, rank, world, npix)
     mode = {"integrate": L.REDUCE_SUM, "volume": L.REDUCE_VOLUME}[w["reduction"]]
     with warnings.catch_warnings():
         warnings.simplefilter("ignore")
         pc = vt.ProjectionCloud(w["pos"], w["fields"], boundbox=w["boundbox"])
     lib = pc._cloud._lib
     h = pc._cloud._h
+    build_cold = pc._cloud.info().tree_build_ms
+    pc._cloud.buildTree()   # warm: module loading and CUB scratch already done
     info = pc._cloud.info()
     nf = int(info.nfields)
     nout = 3 if mode == L.REDUCE_VOLUME else nf
@@ -258,7 +333,7 @@ def run_ours(args):
     def fwd(kernel):
         L.check(lib.vt_project_device(h, d_s.data_ptr(), d_e.data_ptr(), n, mode, kernel,
                                       d_out.data_ptr(), stream.cuda_stream, C.byref(st)))
-        return st.crossings, st.walk_ms, st.fp64_resolves, st.queries
+        return st.crossings, st.walk_ms
 
     def bwd():
         L.check(lib.vt_project_adjoint_device(h, d_s.data_ptr(), d_e.data_ptr(), n, mode,
@@ -266,17 +341,13 @@ def run_ours(args):
                                               d_grad.data_ptr(), stream.cuda_stream))
 
     # forward with a segment tape + scatter adjoint (the autograd path of
-    # 'integrate' and 'volume')
+    # 'integrate' and 'volume'), with any walk kernel
     tape = L.Tape(lib, h)
-    taped = mode in (L.REDUCE_SUM, L.REDUCE_VOLUME)
 
-    def fwd_tape():
-        if not taped:
-            fwd(L.KERNEL_AUTO)
-            return
+    def fwd_tape(kernel):
         L.check(lib.vt_project_device_tape(h, tape.h, d_s.data_ptr(), d_e.data_ptr(), n, mode,
-                                           L.KERNEL_AUTO, d_out.data_ptr(),
-                                           stream.cuda_stream, C.byref(st)))
+                                           kernel, d_out.data_ptr(), stream.cuda_stream,
+                                           C.byref(st)))
 
     def bwd_tape():
         L.check(lib.vt_tape_adjoint_device(h, tape.h, d_s.data_ptr(), d_e.data_ptr(), n, mode,
@@ -286,6 +357,7 @@ def run_ours(args):
     def barrier():
         torch.cuda.synchronize(dev)
         if world > 1:
+            import torch.distributed as dist
             dist.barrier()
         torch.cuda.synchronize(dev)
 
@@ -304,141 +376,186 @@ def run_ours(args):
             ms.append(e0.elapsed_time(e1))
         return ms
 
-    def reduce_max(x):
+    def reduce(x, op):
         if world == 1:
             return x
+        import torch.distributed as dist
         t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=op)
         return float(t.item())
 
-    def reduce_sum(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    def leg(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        barrier()
+        ms = timed(fn, steps)
+        barrier()
+        import torch.distributed as dist
+        return reduce(sum(ms), dist.ReduceOp.MAX if world > 1 else None)
 
-    K, W = args.steps, args.warmup
+    def rate(t_ms, steps):
+        return tot_cross * steps / (t_ms / 1e3) / 1e6
+
     # --- autotune (outside the timed region): the AUTO kernel and the
     # shared-memory tree depth from timings on a sample of this workload's rays
     tune = pc.autotune(S, E, reduction={L.REDUCE_VOLUME: "volume"}.get(mode, "integrate"))
     auto_kernel = tune["kernel"] if n >= tune["sample_rays"] else (
         "batched" if n < 65536 else "thread_fp32")
 
-    # --- forward, batched kernel (the headline)
+    # --- forward, batched kernel (the headline), clocks sampled meanwhile
     for _ in range(W):
         fwd(L.KERNEL_AUTO)
     barrier()
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(int(str(dev).split(":")[-1]))
     sampler.start()
     walk_ms = []
 
     def f_b():
-        c, wm, _, _ = fwd(L.KERNEL_AUTO)
-        walk_ms.append(wm)
+        walk_ms.append(fwd(L.KERNEL_AUTO)[1])
 
     fwd_ms = timed(f_b, K)
     barrier()
     clocks = sampler.stop()
-    crossings, _, resolves, queries = fwd(L.KERNEL_AUTO)
-    t_fwd = reduce_max(sum(fwd_ms))
-    tot_cross = reduce_sum(float(crossings))
-    value = tot_cross * K / (t_fwd / 1e3) / 1e6
+    crossings, _ = fwd(L.KERNEL_AUTO)
+    img_auto = d_out.clone()
+    import torch.distributed as dist
+    t_fwd = reduce(sum(fwd_ms), dist.ReduceOp.MAX if world > 1 else None)
+    tot_cross = reduce(float(crossings), dist.ReduceOp.SUM if world > 1 else None)
+    value = rate(t_fwd, K)
 
-    # --- forward + adjoint (taped forward, scatter adjoint)
-    for _ in range(max(2, W // 2)):
-        fwd_tape()
-        bwd_tape()
-    barrier()
-    fb_ms = timed(lambda: (fwd_tape(), bwd_tape()), K)
-    barrier()
-    t_fb = reduce_max(sum(fb_ms))
-    fb_value = tot_cross * K / (t_fb / 1e3) / 1e6
+    taped = mode in (L.REDUCE_SUM, L.REDUCE_VOLUME)
+    # --- forward + adjoint: taped forward (AUTO) + scatter adjoint
+    t_fb = leg(lambda: (fwd_tape(L.KERNEL_AUTO), bwd_tape()), K, max(2, W // 2))
+    fb_value = rate(t_fb, K)
     tape_entries = int(lib.vt_tape_size(tape.h))
-
-    # --- forward + adjoint that re-walks the rays (no tape)
-    kp = max(2, K // 2)
-    fwd(L.KERNEL_AUTO)
-    bwd()
-    barrier()
-    rw_ms = timed(lambda: (fwd(L.KERNEL_AUTO), bwd()), kp)
-    barrier()
-    t_rw = reduce_max(sum(rw_ms))
-    rw_value = tot_cross * kp / (t_rw / 1e3) / 1e6
-
+    # --- forward + adjoint that re-walks the rays (no tape), AUTO kernel
+    t_rw = leg(lambda: (fwd(L.KERNEL_AUTO), bwd()), kp, wp)
+    rw_value = rate(t_rw, kp)
     # --- the batched kernel with the bounded FP64 k-NN
-    fwd(L.KERNEL_BATCHED_FP64)
-    barrier()
-    f64_ms = timed(lambda: fwd(L.KERNEL_BATCHED_FP64), kp)
-    barrier()
-    t_f64 = reduce_max(sum(f64_ms))
-    f64_value = tot_cross * kp / (t_f64 / 1e3) / 1e6
-
-    # --- the plain kernel's own forward + adjoint (re-walk, plain kernel)
-    pc._cloud.set_param(L.PARAM_ADJOINT_KERNEL, L.KERNEL_PLAIN_FP64)
-    fwd(L.KERNEL_PLAIN_FP64)
-    bwd()
-    barrier()
-    pfb_ms = timed(lambda: (fwd(L.KERNEL_PLAIN_FP64), bwd()), kp)
-    barrier()
-    pc._cloud.set_param(L.PARAM_ADJOINT_KERNEL, L.KERNEL_AUTO)
-    t_pfb = reduce_max(sum(pfb_ms))
-    pfb_value = tot_cross * kp / (t_pfb / 1e3) / 1e6
-
+    t_f64 = leg(lambda: fwd(L.KERNEL_BATCHED_FP64), kp, wp)
+    f64_value = rate(t_f64, kp)
     # --- plain FP64 one-ray-per-thread kernel (the baseline kernel)
+    t_pl = leg(lambda: fwd(L.KERNEL_PLAIN_FP64), kp, wp)
+    pl_value = rate(t_pl, kp)
     fwd(L.KERNEL_PLAIN_FP64)
-    barrier()
-    pl_ms = timed(lambda: fwd(L.KERNEL_PLAIN_FP64), kp)
-    barrier()
-    t_pl = reduce_max(sum(pl_ms))
-    pl_value = tot_cross * kp / (t_pl / 1e3) / 1e6
+    img_plain = d_out.clone()
+    # --- the plain kernel's forward + adjoint, like for like: taped plain
+    # forward + the same scatter adjoint
+    t_ptb = leg(lambda: (fwd_tape(L.KERNEL_PLAIN_FP64), bwd_tape()), kp, wp)
+    ptb_value = rate(t_ptb, kp)
+    # --- ... and with the plain kernel re-walking for the adjoint
+    pc._cloud.set_param(L.PARAM_ADJOINT_KERNEL, L.KERNEL_PLAIN_FP64)
+    t_pfb = leg(lambda: (fwd(L.KERNEL_PLAIN_FP64), bwd()), kp, wp)
+    pc._cloud.set_param(L.PARAM_ADJOINT_KERNEL, L.KERNEL_AUTO)
+    pfb_value = rate(t_pfb, kp)
 
-    # --- end to end through the C ABI with host buffers (pinned)
-    hS = torch.from_numpy(S).pin_memory().numpy()
-    hE = torch.from_numpy(E).pin_memory().numpy()
-    hO = torch.empty((n, nout), dtype=torch.float64).pin_memory().numpy()
-    st2 = L.Stats()
-
-    def e2e_step():
-        L.check(lib.vt_project(h, L.dptr(hS), L.dptr(hE), n, mode, L.KERNEL_AUTO, L.dptr(hO),
-                               C.byref(st2)))
-
-    e2e_step()
-    barrier()
-    e2e_s = []
-    for i in range(K):
-        flush.fill_(i & 0xff)
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        e2e_step()
-        e2e_s.append(time.perf_counter() - t0)
-    barrier()
-    t_e2e = reduce_max(sum(e2e_s))
-    e2e_value = tot_cross * K / t_e2e / 1e6
+    rec = {
+        "workload": f"{name}: {w['meta']}", "rays_per_gpu": n, "reduction": w["reduction"],
+        "crossings_per_step": int(tot_cross), "value": round(value, 4),
+        "ms_per_step": round(t_fwd / K, 3), "steps": K, "warmup": W,
+        "baseline_steps": kp, "baseline_warmup": wp,
+        "rays_per_s": round(n * world * K / (t_fwd / 1e3), 1),
+        "kernel": f"VT_KERNEL_AUTO = {auto_kernel}", "autotune": tune,
+        "fwd_bwd_mcrossings_per_s": round(fb_value, 4),
+        "fwd_bwd_adjoint": (f"segment tape ({48 if mode == L.REDUCE_VOLUME else 16} "
+                            "B/crossing) + scatter" if taped and tape_entries > 0
+                            else "re-walk"),
+        "fwd_bwd_rewalk_mcrossings_per_s": round(rw_value, 4),
+        "bounded_fp64_mcrossings_per_s": round(f64_value, 4),
+        "plain_fp64_mcrossings_per_s": round(pl_value, 4),
+        "speedup_vs_plain_fp64": round(value / pl_value, 3),
+        "plain_fp64_taped_fwd_bwd_mcrossings_per_s": round(ptb_value, 4),
+        "fwd_bwd_speedup_vs_plain_fp64_taped": round(fb_value / ptb_value, 3),
+        "plain_fp64_fwd_bwd_mcrossings_per_s": round(pfb_value, 4),
+        "fwd_bwd_speedup_vs_plain_fp64_rewalk": round(fb_value / pfb_value, 3),
+        "tree_build_ms": {"first": round(build_cold, 2), "warm": round(info.tree_build_ms, 2)},
+        "clocks": clocks,
+    }
 
     # --- roofline of the dominant kernel (k_batched + the tiny k_slow)
-    bx = BX.get(args.config)
-    peak, peak_src = None, None
+    bx = BX.get(name)
     mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(mp):
         with open(mp) as f:
-            peak = float(json.load(f)["hbm_gbs"])
-        peak_src = "measured"
+            peak, peak_src = float(json.load(f)["hbm_gbs"]), "measured"
     else:
         peak, peak_src = 6650.0, "fallback"
     launch_ms = statistics.mean(walk_ms) if walk_ms else None
-    roof = None
     if bx and launch_ms:
         achieved = crossings * bx / (launch_ms / 1e3) / 1e9
-        # (measured for the guarded-FP32 kernel)
-        dpc = DRAM_BYTES_PER_CROSSING.get(args.config) if auto_kernel == "thread_fp32" else None
-        traffic = round(dpc * crossings) if dpc else None
-        roof = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": traffic,
-                "peak_source": peak_src, "bytes_per_crossing": bx,
-                "kernel": {"thread_fp32": "k_batched (guarded-FP32 k-NN, coherent ray order)",
-                           "batched_fp64": "k_batched (bounded FP64 k-NN, coherent ray order)",
-                           "batched": "k_warp (one ray per warp)"}.get(auto_kernel, auto_kernel)}
+        dpc = DRAM_BYTES_PER_CROSSING.get((name, auto_kernel))
+        rec["roofline"] = {
+            "bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "traffic": round(dpc * crossings) if dpc else None,
+            "peak_source": peak_src, "bytes_per_crossing": bx,
+            "launch_ms": round(launch_ms, 3),
+            "kernel": {"thread_fp32": "k_batched (guarded-FP32 k-NN, coherent ray order)",
+                       "batched_fp64": "k_batched (bounded FP64 k-NN, coherent ray order)",
+                       "batched": "k_warp (one ray per warp)"}.get(auto_kernel, auto_kernel)}
+
+    # --- parity (outside the timed region; one process: rank 0 of N = 1)
+    if rank == 0 and world == 1:
+        par = {"image_bit_identical_to_plain_fp64": bool(torch.equal(img_auto, img_plain))}
+        try:
+            sp, idx, o = oracle_sample_parity(w, pc, auto_kernel)
+            par.update(sp)
+            got = img_auto.cpu().numpy()[idx].reshape(len(idx), -1)
+            par["image_rows_bit_identical_to_oracle"] = bool(np.array_equal(got, o))
+        except Exception as e:   # keep the timing line
+            par["oracle_error"] = str(e)
+        rec["parity"] = par
+        try:
+            rec["counters"] = counters_run(w, L.KERNEL_THREAD_FP32, tune["smem_levels"], mode)
+        except Exception as e:
+            rec["counters"] = {"error": str(e)}
+
+    e2e = None
+    if full:
+        # --- end to end through the C ABI with host buffers (pinned)
+        hS = torch.from_numpy(S).pin_memory().numpy()
+        hE = torch.from_numpy(E).pin_memory().numpy()
+        hO = torch.empty((n, nout), dtype=torch.float64).pin_memory().numpy()
+        st2 = L.Stats()
+
+        def e2e_step():
+            L.check(lib.vt_project(h, L.dptr(hS), L.dptr(hE), n, mode, L.KERNEL_AUTO,
+                                   L.dptr(hO), C.byref(st2)))
+
+        e2e_step()
+        barrier()
+        e2e_s = []
+        for i in range(K):
+            flush.fill_(i & 0xff)
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            e2e_step()
+            e2e_s.append(time.perf_counter() - t0)
+        barrier()
+        t_e2e = reduce(sum(e2e_s), dist.ReduceOp.MAX if world > 1 else None)
+        e2e = {"value": round(tot_cross * K / t_e2e / 1e6, 4), "unit": UNIT,
+               "h2d_bytes_per_step": int(2 * n * 3 * 8), "d2h_bytes_per_step": int(n * nout * 8)}
+    del tape
+    return rec, e2e, w
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from vortrace_b200 import _lib as L
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    L.load().vt_set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    K, W = args.steps, args.warmup
+    rec, e2e, w = measure(args.config, args, rank, world, dev, K, W, npix=args.npix)
+    n = rec["rays_per_gpu"]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -450,42 +567,49 @@ def run_ours(args):
         except Exception as e:  # keep the GPU line even if the CPU leg fails
             cpu = {"value": None, "unit": UNIT, "cores": host_cores(), "kind": "unavailable",
                    "sample": f"CPU baseline failed: {e}"}
+    del w
+
+    target = None
+    if rank == 0 and world == 1 and args.target and args.target != args.config:
+        # the >= 3x target configuration (16M-point nested cloud), fewer steps
+        try:
+            target, _, _ = measure(args.target, args, 0, 1, dev, args.target_steps, 3,
+                                   kp=2, wp=1, full=False)
+        except Exception as e:
+            target = {"workload": args.target, "error": str(e)}
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
-            "steps": K, "warmup": W, "ms_per_step": round(t_fwd / K, 3),
+            "metric": METRIC, "value": rec["value"], "unit": UNIT, "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": rec["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"{args.config}: {w['meta']}", "rays_per_gpu": n,
-                       "crossings_per_step": int(tot_cross), "reduction": w["reduction"],
+            "config": {"workload": rec["workload"], "rays_per_gpu": n,
+                       "crossings_per_step": rec["crossings_per_step"],
+                       "reduction": rec["reduction"],
                        "l2": "flushed before every timed step (256 MB write)",
-                       "tree_build_ms": round(info.tree_build_ms, 2),
+                       "tree_build_ms": rec["tree_build_ms"],
                        "parallelism": f"rays sharded by view, {world} rank(s)"},
-            "fwd_bwd_mcrossings_per_s": round(fb_value, 4),
-            "fwd_bwd_adjoint": (f"segment tape ({48 if mode == L.REDUCE_VOLUME else 16} "
-                                "B/crossing) + scatter" if taped and tape_entries > 0
-                                else "re-walk"),
-            "fwd_bwd_rewalk_mcrossings_per_s": round(rw_value, 4),
-            "kernel": f"VT_KERNEL_AUTO = {auto_kernel}",
-            "autotune": tune,
-            "bounded_fp64_mcrossings_per_s": round(f64_value, 4),
-            "plain_fp64_mcrossings_per_s": round(pl_value, 4),
-            "speedup_vs_plain_fp64": round(value / pl_value, 3),
-            "plain_fp64_fwd_bwd_mcrossings_per_s": round(pfb_value, 4),
-            "fwd_bwd_speedup_vs_plain_fp64_fwd_bwd": round(fb_value / pfb_value, 3),
-            "rays_per_s": round(n * world * K / (t_fwd / 1e3), 1),
-            "fp64_resolve_fraction": round(resolves / max(1, queries), 6),
-            "e2e": {"value": round(e2e_value, 4), "unit": UNIT,
-                    "h2d_bytes_per_step": int(2 * n * 3 * 8),
-                    "d2h_bytes_per_step": int(n * nout * 8)},
-            # per timed forward step: k_ray_keys, k_batched, k_slow (CUB's
+        }
+        for k in ("fwd_bwd_mcrossings_per_s", "fwd_bwd_adjoint",
+                  "fwd_bwd_rewalk_mcrossings_per_s", "kernel", "autotune",
+                  "bounded_fp64_mcrossings_per_s", "plain_fp64_mcrossings_per_s",
+                  "speedup_vs_plain_fp64", "plain_fp64_taped_fwd_bwd_mcrossings_per_s",
+                  "fwd_bwd_speedup_vs_plain_fp64_taped", "plain_fp64_fwd_bwd_mcrossings_per_s",
+                  "fwd_bwd_speedup_vs_plain_fp64_rewalk", "rays_per_s", "parity", "counters"):
+            if k in rec:
+                line[k] = rec[k]
+        line.update({
+            "e2e": e2e,
+            # per timed forward step: k_ray_keys, the walk kernel, k_slow (CUB's
             # radix-sort kernels of the ray order not counted)
             "gpu_launches": 3 * K,
-            "roofline": roof,
+            "roofline": rec.get("roofline"),
             "cpu_baseline": cpu,
-            "clocks": clocks,
-        }
+            "clocks": rec["clocks"],
+        })
+        if target is not None:
+            line["target_config"] = target
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -504,6 +628,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--npix", type=int, default=None,
                     help="override the grid resolution (smaller profiling case)")
+    ap.add_argument("--target", default="nested_16m",
+                    help="second workload reported as target_config at N=1 ('' to skip)")
+    ap.add_argument("--target-steps", type=int, default=3)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -113,12 +113,16 @@ typedef struct {
   uint64_t slow_rays;     /* rays finished by the degenerate-geometry kernel */
   uint64_t max_stack;     /* deepest pending-point stack seen                */
   double walk_ms;         /* device time of the walk launch(es)               */
-  uint64_t search_steps;  /* node groups expanded (warp-cooperative search)  */
+  uint64_t search_steps;  /* nodes / node groups the searches expanded        */
   uint64_t fp64_checks;   /* FP64 re-checks of points passing the FP32 test  */
+                          /* (these three: the library built with
+                             VT_BATCHED_COUNTERS=1, or k_warp)               */
   uint64_t cache_refreshes; /* neighbourhood-cache refills (batched kernel)  */
   uint64_t cache_hits;    /* split queries answered from the cache           */
   uint64_t ties;          /* 1-NN queries whose nearest distance was exactly
                              shared, answered in the reference's order       */
+  uint64_t fp32_queries;  /* guarded-FP32 split queries (counters build)     */
+  uint64_t fp64_check_queries; /* ... with at least one FP64 re-check        */
 } vt_stats;
 
 /* ---- library ----------------------------------------------------------- */

@@ -80,7 +80,8 @@ class Stats(C.Structure):
                 ("max_stack", C.c_uint64), ("walk_ms", C.c_double),
                 ("search_steps", C.c_uint64), ("fp64_checks", C.c_uint64),
                 ("cache_refreshes", C.c_uint64), ("cache_hits", C.c_uint64),
-                ("ties", C.c_uint64)]
+                ("ties", C.c_uint64), ("fp32_queries", C.c_uint64),
+                ("fp64_check_queries", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -106,83 +107,93 @@ def load(path: str | None = None):
     with _lock:
         if _lib is not None:
             return _lib
-        p = path or LIB_PATH
-        if not os.path.exists(p):
-            raise ImportError(
-                f"libvortrace_b200.so not found at {p}; build it with "
-                "`python -m vortrace_b200.build` (nvcc, sm_100a)")
-        L = C.CDLL(p)
-        dp = C.POINTER(C.c_double)
-        i64p = C.POINTER(C.c_int64)
-        vp = C.c_void_p
-        u64 = C.c_uint64
-        L.vt_abi_version.restype = C.c_int
-        L.vt_last_error.restype = C.c_char_p
-        L.vt_set_verbose.argtypes = [C.c_int]
-        L.vt_get_verbose.restype = C.c_int
-        L.vt_set_warning_callback.argtypes = [_WARN_CB_T]
-        L.vt_set_device.argtypes = [C.c_int]
-        L.vt_cloud_create.argtypes = [dp, u64, dp, u64, u64, dp, dp, u64, C.c_int,
-                                      C.POINTER(vp)]
-        L.vt_cloud_build_tree.argtypes = [vp]
-        L.vt_cloud_build_tie_tree.argtypes = [vp]
-        L.vt_cloud_set_param.argtypes = [vp, C.c_int, C.c_int64]
-        L.vt_cloud_set_fields.argtypes = [vp, dp]
-        L.vt_cloud_set_fields_device.argtypes = [vp, vp, vp]
-        L.vt_cloud_get_info.argtypes = [vp, C.POINTER(CloudInfo)]
-        L.vt_cloud_orig_ids.argtypes = [vp, i64p, u64]
-        L.vt_cloud_destroy.argtypes = [vp]
-        L.vt_cloud_destroy.restype = None
-        L.vt_knn.argtypes = [vp, dp, u64, C.c_int, i64p, dp]
-        L.vt_project.argtypes = [vp, dp, dp, u64, C.c_int, C.c_int, dp, C.POINTER(Stats)]
-        L.vt_project_device.argtypes = [vp, vp, vp, u64, C.c_int, C.c_int, vp, vp,
-                                        C.POINTER(Stats)]
-        L.vt_project_device_noalloc.argtypes = [vp, vp, vp, u64, C.c_int, vp, vp]
-        L.vt_project_detailed.argtypes = [vp, dp, dp, u64, C.c_int, dp, i64p, C.POINTER(vp)]
-        L.vt_segments_count.argtypes = [vp]
-        L.vt_segments_count.restype = u64
-        L.vt_segments_copy.argtypes = [vp, i64p, dp, dp]
-        L.vt_segments_free.argtypes = [vp]
-        L.vt_segments_free.restype = None
-        L.vt_project_adjoint.argtypes = [vp, dp, dp, u64, C.c_int, dp, dp, dp]
-        L.vt_project_adjoint_device.argtypes = [vp, vp, vp, u64, C.c_int, vp, vp, vp, vp]
-        L.vt_tape_create.argtypes = [vp, C.POINTER(vp)]
-        L.vt_tape_destroy.argtypes = [vp]
-        L.vt_tape_destroy.restype = None
-        L.vt_slice.argtypes = [vp, C.POINTER(u64), dp, C.c_double, dp]
-        L.vt_cloud_autotune.argtypes = [vp, dp, dp, u64, C.c_int, u64, C.POINTER(TuneResult)]
-        L.vt_graph_create.argtypes = [vp, vp, vp, u64, C.c_int, C.c_int, vp, C.POINTER(vp)]
-        L.vt_graph_launch.argtypes = [vp, vp]
-        L.vt_cloud_tree_save.argtypes = [vp, vp, u64, C.POINTER(u64)]
-        L.vt_cloud_tree_load.argtypes = [vp, vp, u64]
-        L.vt_graph_finish.argtypes = [vp, vp, C.POINTER(Stats)]
-        L.vt_graph_destroy.argtypes = [vp]
-        L.vt_graph_destroy.restype = None
-        L.vt_brute_projection.argtypes = [vp, C.POINTER(u64), dp, C.c_int, dp]
-        L.vt_grid_rays_device.argtypes = [dp, u64, u64, dp, vp, vp, vp]
-        L.vt_project_grid.argtypes = [vp, dp, u64, u64, dp, C.c_int, C.c_int, dp,
-                                      C.POINTER(Stats)]
-        L.vt_tape_size.argtypes = [vp]
-        L.vt_tape_size.restype = u64
-        L.vt_project_device_tape.argtypes = [vp, vp, vp, vp, u64, C.c_int, C.c_int, vp, vp,
-                                             C.POINTER(Stats)]
-        L.vt_tape_adjoint_device.argtypes = [vp, vp, vp, vp, u64, C.c_int, vp, vp, vp, vp]
-        for name in ("vt_cloud_create", "vt_cloud_build_tree", "vt_cloud_build_tie_tree",
-                     "vt_cloud_set_param",
-                     "vt_cloud_set_fields", "vt_cloud_set_fields_device",
-                     "vt_cloud_get_info", "vt_cloud_orig_ids", "vt_knn", "vt_project",
-                     "vt_project_device", "vt_project_device_noalloc", "vt_project_detailed",
-                     "vt_segments_copy",
-                     "vt_project_adjoint", "vt_project_adjoint_device", "vt_set_device",
-                     "vt_tape_create", "vt_project_device_tape", "vt_tape_adjoint_device",
-                     "vt_slice", "vt_brute_projection", "vt_cloud_autotune",
-                     "vt_graph_create", "vt_graph_launch", "vt_graph_finish",
-                     "vt_cloud_tree_save", "vt_cloud_tree_load", "vt_grid_rays_device",
-                     "vt_project_grid"):
-            getattr(L, name).restype = C.c_int
-        L.vt_set_warning_callback(_warn_cb)
-        _lib = L
-        return L
+        _lib = _open(path or LIB_PATH)
+        return _lib
+
+
+def load_variant(path: str):
+    """A separately loaded build of the library (e.g. the one with the search
+    counters compiled in, libvortrace_b200_counters.so): its own handles,
+    streams and device memory; not the default library of the package."""
+    return _open(path)
+
+
+def _open(p: str):
+    if not os.path.exists(p):
+        raise ImportError(
+            f"{os.path.basename(p)} not found at {p}; build it with "
+            "`python -m vortrace_b200.build` (nvcc, sm_100a)")
+    L = C.CDLL(p)
+    dp = C.POINTER(C.c_double)
+    i64p = C.POINTER(C.c_int64)
+    vp = C.c_void_p
+    u64 = C.c_uint64
+    L.vt_abi_version.restype = C.c_int
+    L.vt_last_error.restype = C.c_char_p
+    L.vt_set_verbose.argtypes = [C.c_int]
+    L.vt_get_verbose.restype = C.c_int
+    L.vt_set_warning_callback.argtypes = [_WARN_CB_T]
+    L.vt_set_device.argtypes = [C.c_int]
+    L.vt_cloud_create.argtypes = [dp, u64, dp, u64, u64, dp, dp, u64, C.c_int,
+                                  C.POINTER(vp)]
+    L.vt_cloud_build_tree.argtypes = [vp]
+    L.vt_cloud_build_tie_tree.argtypes = [vp]
+    L.vt_cloud_set_param.argtypes = [vp, C.c_int, C.c_int64]
+    L.vt_cloud_set_fields.argtypes = [vp, dp]
+    L.vt_cloud_set_fields_device.argtypes = [vp, vp, vp]
+    L.vt_cloud_get_info.argtypes = [vp, C.POINTER(CloudInfo)]
+    L.vt_cloud_orig_ids.argtypes = [vp, i64p, u64]
+    L.vt_cloud_destroy.argtypes = [vp]
+    L.vt_cloud_destroy.restype = None
+    L.vt_knn.argtypes = [vp, dp, u64, C.c_int, i64p, dp]
+    L.vt_project.argtypes = [vp, dp, dp, u64, C.c_int, C.c_int, dp, C.POINTER(Stats)]
+    L.vt_project_device.argtypes = [vp, vp, vp, u64, C.c_int, C.c_int, vp, vp,
+                                    C.POINTER(Stats)]
+    L.vt_project_device_noalloc.argtypes = [vp, vp, vp, u64, C.c_int, vp, vp]
+    L.vt_project_detailed.argtypes = [vp, dp, dp, u64, C.c_int, dp, i64p, C.POINTER(vp)]
+    L.vt_segments_count.argtypes = [vp]
+    L.vt_segments_count.restype = u64
+    L.vt_segments_copy.argtypes = [vp, i64p, dp, dp]
+    L.vt_segments_free.argtypes = [vp]
+    L.vt_segments_free.restype = None
+    L.vt_project_adjoint.argtypes = [vp, dp, dp, u64, C.c_int, dp, dp, dp]
+    L.vt_project_adjoint_device.argtypes = [vp, vp, vp, u64, C.c_int, vp, vp, vp, vp]
+    L.vt_tape_create.argtypes = [vp, C.POINTER(vp)]
+    L.vt_tape_destroy.argtypes = [vp]
+    L.vt_tape_destroy.restype = None
+    L.vt_slice.argtypes = [vp, C.POINTER(u64), dp, C.c_double, dp]
+    L.vt_cloud_autotune.argtypes = [vp, dp, dp, u64, C.c_int, u64, C.POINTER(TuneResult)]
+    L.vt_graph_create.argtypes = [vp, vp, vp, u64, C.c_int, C.c_int, vp, C.POINTER(vp)]
+    L.vt_graph_launch.argtypes = [vp, vp]
+    L.vt_cloud_tree_save.argtypes = [vp, vp, u64, C.POINTER(u64)]
+    L.vt_cloud_tree_load.argtypes = [vp, vp, u64]
+    L.vt_graph_finish.argtypes = [vp, vp, C.POINTER(Stats)]
+    L.vt_graph_destroy.argtypes = [vp]
+    L.vt_graph_destroy.restype = None
+    L.vt_brute_projection.argtypes = [vp, C.POINTER(u64), dp, C.c_int, dp]
+    L.vt_grid_rays_device.argtypes = [dp, u64, u64, dp, vp, vp, vp]
+    L.vt_project_grid.argtypes = [vp, dp, u64, u64, dp, C.c_int, C.c_int, dp,
+                                  C.POINTER(Stats)]
+    L.vt_tape_size.argtypes = [vp]
+    L.vt_tape_size.restype = u64
+    L.vt_project_device_tape.argtypes = [vp, vp, vp, vp, u64, C.c_int, C.c_int, vp, vp,
+                                         C.POINTER(Stats)]
+    L.vt_tape_adjoint_device.argtypes = [vp, vp, vp, vp, u64, C.c_int, vp, vp, vp, vp]
+    for name in ("vt_cloud_create", "vt_cloud_build_tree", "vt_cloud_build_tie_tree",
+                 "vt_cloud_set_param",
+                 "vt_cloud_set_fields", "vt_cloud_set_fields_device",
+                 "vt_cloud_get_info", "vt_cloud_orig_ids", "vt_knn", "vt_project",
+                 "vt_project_device", "vt_project_device_noalloc", "vt_project_detailed",
+                 "vt_segments_copy",
+                 "vt_project_adjoint", "vt_project_adjoint_device", "vt_set_device",
+                 "vt_tape_create", "vt_project_device_tape", "vt_tape_adjoint_device",
+                 "vt_slice", "vt_brute_projection", "vt_cloud_autotune",
+                 "vt_graph_create", "vt_graph_launch", "vt_graph_finish",
+                 "vt_cloud_tree_save", "vt_cloud_tree_load", "vt_grid_rays_device",
+                 "vt_project_grid"):
+        getattr(L, name).restype = C.c_int
+    L.vt_set_warning_callback(_warn_cb)
+    return L
 
 
 class VortraceError(RuntimeError):
@@ -193,11 +204,12 @@ class VortraceError(RuntimeError):
         self.code = code
 
 
-def check(rc: int):
-    """Raise the Python exception the reference raises for this status."""
+def check(rc: int, lib=None):
+    """Raise the Python exception the reference raises for this status
+    (``lib``: the library that returned it, default the package's)."""
     if rc == VT_OK:
         return
-    msg = (_lib.vt_last_error() or b"").decode(errors="replace")
+    msg = ((lib or _lib).vt_last_error() or b"").decode(errors="replace")
     if rc == VT_ERR_INVALID:
         raise ValueError(msg)
     if rc == VT_ERR_NOMEM:

@@ -5,7 +5,11 @@
 Every .cu file under csrc/ is compiled for ``-gencode
 arch=compute_100a,code=sm_100a`` with ``--fmad=false`` (FP64 expressions must
 round like the reference's x86-64 build) and linked into
-``vortrace_b200/libvortrace_b200.so`` next to this file.
+``vortrace_b200/libvortrace_b200.so`` next to this file.  A second build with
+the search counters of the batched kernel compiled in
+(``-DVT_BATCHED_COUNTERS=1``: nodes visited, FP64 re-checks, queries with a
+re-check) goes to ``libvortrace_b200_counters.so``; the benchmark reads its
+counters in a launch outside the timed region.
 """
 from __future__ import annotations
 
@@ -20,6 +24,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libvortrace_b200.so")
+LIB_COUNTERS = os.path.join(HERE, "libvortrace_b200_counters.so")
+COUNTER_DEFINES = ("VT_BATCHED_COUNTERS=1",)
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -53,10 +59,10 @@ def _deps():
                                                  os.path.abspath(__file__)]
 
 
-def up_to_date() -> bool:
-    if not os.path.exists(LIB):
+def up_to_date(lib: str = LIB) -> bool:
+    if not os.path.exists(lib):
         return False
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     return all(os.path.getmtime(d) <= t for d in _deps())
 
 
@@ -65,9 +71,10 @@ def build(force: bool = False, ptxas_verbose: bool = False, jobs: int = 0,
     """Compile and link; ``out``/``defines`` build a variant elsewhere (for
     tuning sweeps, e.g. defines=("VT_BATCHED_MINB=6",))."""
     lib = out or LIB
-    if out is None and not defines and not force and up_to_date():
-        return LIB
-    bdir = BUILD if out is None else lib + ".objs"
+    if not force and (out is None or out == LIB_COUNTERS) and up_to_date(lib):
+        return lib
+    bdir = BUILD if out is None else (BUILD + "_counters" if out == LIB_COUNTERS
+                                      else lib + ".objs")
     os.makedirs(bdir, exist_ok=True)
     cc = nvcc()
     objs, procs = [], []
@@ -96,12 +103,20 @@ def build(force: bool = False, ptxas_verbose: bool = False, jobs: int = 0,
     return lib
 
 
+def build_counters(force: bool = False) -> str:
+    """The library with the batched kernel's search counters compiled in."""
+    return build(force=force, out=LIB_COUNTERS, defines=COUNTER_DEFINES)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose-ptxas", action="store_true")
+    ap.add_argument("--no-counters", action="store_true")
     a = ap.parse_args()
     print(build(force=a.force, ptxas_verbose=a.verbose_ptxas))
+    if not a.no_counters:
+        print(build_counters(force=a.force))
 
 
 if __name__ == "__main__":

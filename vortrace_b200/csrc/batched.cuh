@@ -42,8 +42,11 @@ constexpr int kBatchStack = 32;
 #define VT_LEAF_BATCH64 4
 #endif
 // 1: the launch statistics also count the tree nodes the searches visit
-// (search_steps) and the FP64 re-checks of FP32-passing points
-// (fp64_checks); off by default, the counters cost registers
+// (search_steps), the FP64 re-checks of FP32-passing points other than the
+// two cells of the split (fp64_checks), the guarded-FP32 split queries
+// (fp32_queries) and those among them with at least one such re-check
+// (recheck_queries); off by default, the counters cost registers (a build
+// of the library with them on is made beside the default one)
 #ifndef VT_BATCHED_COUNTERS
 #define VT_BATCHED_COUNTERS 0
 #endif
@@ -183,7 +186,8 @@ template <class F>
 __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, double qx,
                                              double qy, double qz, int cid, int nid, double dc,
                                              double dn, double R, double G, KnnList<3>& res,
-                                             unsigned& nvisit, unsigned& nverify) {
+                                             unsigned& nvisit, unsigned& nverify,
+                                             unsigned& nqverify) {
   const float q0 = __double2float_rn(dsub(qx, c.origin[0]));
   const float q1 = __double2float_rn(dsub(qy, c.origin[1]));
   const float q2 = __double2float_rn(dsub(qz, c.origin[2]));
@@ -308,6 +312,7 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
   }
   nvisit += visits;
   nverify += ver;
+  nqverify += ver > 0;
 }
 
 // A bounded result B (all points with d < R, at most 3, exact order) gives
@@ -431,6 +436,7 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
   AdjSink<MODE, NF> adj;
   // lane counters
   unsigned n_rays = 0, n_cross = 0, n_q = 0, n_res = 0, n_visit = 0, n_ver = 0, max_sp = 0;
+  unsigned n_qver = 0, n_q32 = 0;
 
   for (;;) {
     // ---- refill idle lanes from the work queue
@@ -571,7 +577,8 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
       ++n_q;
       if (G32) {
         const double G = guard_band(R, q_err);
-        knn3_guarded(c, f32, qx, qy, qz, cur, nxt, dc, dn, R, G, r, n_visit, n_ver);
+        knn3_guarded(c, f32, qx, qy, qz, cur, nxt, dc, dn, R, G, r, n_visit, n_ver, n_qver);
+        ++n_q32;
       } else {
         r.clear();
         knn64_fetch(c, f64, qx, qy, qz, R, r, n_visit);
@@ -670,6 +677,8 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
 #if VT_BATCHED_COUNTERS
   warp_add(&io.stats->search_steps, n_visit);
   warp_add(&io.stats->fp64_checks, n_ver);
+  warp_add(&io.stats->recheck_queries, n_qver);
+  warp_add(&io.stats->fp32_queries, n_q32);
 #endif
 }
 

@@ -157,6 +157,8 @@ struct DevStats {
   unsigned long long cache_hits;       // split queries answered from the cache
   unsigned long long ties;             // 1-NN queries that met an exact tie
   unsigned long long tie_deferred;     // rays waiting for the reference-order tree
+  unsigned long long recheck_queries;  // guarded-FP32 queries with >= 1 FP64 re-check
+  unsigned long long fp32_queries;     // guarded-FP32 split queries
 };
 
 // Sum a small per-lane value over the active lanes, one atomic per warp.

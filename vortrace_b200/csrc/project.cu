@@ -213,6 +213,8 @@ static int finish_walk(vt_cloud* cl, WalkIO& io, const DevStats& hs, float ms, c
     stats->cache_refreshes = hs.cache_refreshes;
     stats->cache_hits = hs.cache_hits;
     stats->ties = hs.ties;
+    stats->fp32_queries = hs.fp32_queries;
+    stats->fp64_check_queries = hs.recheck_queries;
   }
   if (hs.first_error != ~0ULL) {
     const int64_t ray = (int64_t)(hs.first_error >> 8);
