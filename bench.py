@@ -291,7 +291,11 @@ def counters_run(w, kernel, smem_levels, mode):
             "fp64_rechecks_per_query": round(st.fp64_checks / q32, 4),
             "queries_with_fp64_recheck_fraction": round(st.fp64_check_queries / q32, 6),
             "fp64_full_resolves": int(st.fp64_resolves),
-            "fp64_full_resolve_fraction": round(st.fp64_resolves / max(1, st.queries), 8)}
+            "fp64_full_resolve_fraction": round(st.fp64_resolves / max(1, st.queries), 8),
+            "search_simd_efficiency": round(st.search_lane_steps /
+                                            max(1, 32 * st.search_warp_steps), 4),
+            "trip_cycle_shares": [round(x / max(1, sum(st.trip_cycles)), 4)
+                                  for x in st.trip_cycles]}
 
 
 def measure(name, args, rank, world, dev, K, W, *, kp=None, wp=None, full=True,
@@ -601,9 +605,11 @@ def run_ours(args):
                 line[k] = rec[k]
         line.update({
             "e2e": e2e,
-            # per timed forward step: k_ray_keys, the walk kernel, k_slow (CUB's
-            # radix-sort kernels of the ray order not counted)
-            "gpu_launches": 3 * K,
+            # per timed forward step: k_ray_keys, the walk kernel, k_slow, and
+            # for batches of fewer than 8 x 20 x 148 warps' rays also
+            # k_ray_cost, k_batch_keys and k_permute_batches (longest batches
+            # first); CUB's radix-sort kernels not counted
+            "gpu_launches": (3 + (3 if n < 8 * 20 * 148 * 32 else 0)) * K,
             "roofline": rec.get("roofline"),
             "cpu_baseline": cpu,
             "clocks": rec["clocks"],

@@ -123,6 +123,11 @@ typedef struct {
                              shared, answered in the reference's order       */
   uint64_t fp32_queries;  /* guarded-FP32 split queries (counters build)     */
   uint64_t fp64_check_queries; /* ... with at least one FP64 re-check        */
+  uint64_t trip_cycles[3];  /* counters build, one-ray-per-thread kernel:
+                               warp cycles before / in / after the split
+                               search of each loop trip                     */
+  uint64_t search_warp_steps; /* ... search steps of the warps (longest lane) */
+  uint64_t search_lane_steps; /* ... search steps of all lanes                */
 } vt_stats;
 
 /* ---- library ----------------------------------------------------------- */

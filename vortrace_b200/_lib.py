@@ -81,10 +81,13 @@ class Stats(C.Structure):
                 ("search_steps", C.c_uint64), ("fp64_checks", C.c_uint64),
                 ("cache_refreshes", C.c_uint64), ("cache_hits", C.c_uint64),
                 ("ties", C.c_uint64), ("fp32_queries", C.c_uint64),
-                ("fp64_check_queries", C.c_uint64)]
+                ("fp64_check_queries", C.c_uint64), ("trip_cycles", C.c_uint64 * 3),
+                ("search_warp_steps", C.c_uint64), ("search_lane_steps", C.c_uint64)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["trip_cycles"] = list(self.trip_cycles)
+        return d
 
 
 _lib = None

@@ -438,7 +438,16 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
   unsigned n_rays = 0, n_cross = 0, n_q = 0, n_res = 0, n_visit = 0, n_ver = 0, max_sp = 0;
   unsigned n_qver = 0, n_q32 = 0;
 
+#if VT_BATCHED_COUNTERS
+  // trip profile (lane 0): cycles before the search (refill + walk logic),
+  // in the search, after it (apply + tape); search-loop steps of the
+  // warp (its longest search per trip) and of all lanes
+  unsigned long long cyc_pre = 0, cyc_search = 0, cyc_post = 0, wsteps = 0, lsteps = 0;
+#endif
   for (;;) {
+#if VT_BATCHED_COUNTERS
+    const long long t_trip = clock64();
+#endif
     // ---- refill idle lanes from the work queue
     // a warp takes 32 consecutive rays (of the coherent order) once all its
     // lanes are idle: neighbouring rays visit the same tree nodes, so the
@@ -568,6 +577,10 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
     }
 
     // ---- search (lanes of one kind run the same code)
+#if VT_BATCHED_COUNTERS
+    const long long t_search = clock64();
+    const unsigned visit0 = n_visit;
+#endif
     KnnList<3> r;
     if (qkind == 1) {
       r.clear();
@@ -590,6 +603,20 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
       }
     }
 
+#if VT_BATCHED_COUNTERS
+    const long long t_apply = clock64();
+    {
+      const unsigned my = qkind == 2 ? n_visit - visit0 : 0u;
+      const unsigned mx = __reduce_max_sync(FULL, my);
+      const unsigned sm = __reduce_add_sync(FULL, my);
+      if (lane == 0) {
+        wsteps += mx;
+        lsteps += sm;
+        cyc_pre += (unsigned long long)(t_search - t_trip);
+        cyc_search += (unsigned long long)(t_apply - t_search);
+      }
+    }
+#endif
     // ---- apply
     if (qkind != 0 && r.id[0] < 0) {
       fail(kErrNonFiniteDist);  // squared distances overflowed
@@ -668,6 +695,10 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
     }
     // every lane reaches the end of a trip: write this trip's tape entries
     if constexpr (OUT == kOutTape) red.flush_tape(io);
+#if VT_BATCHED_COUNTERS
+    __syncwarp();
+    if (lane == 0) cyc_post += (unsigned long long)(clock64() - t_apply);
+#endif
   }
   warp_add(&io.stats->rays, n_rays);
   warp_add(&io.stats->crossings, n_cross);
@@ -679,6 +710,13 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
   warp_add(&io.stats->fp64_checks, n_ver);
   warp_add(&io.stats->recheck_queries, n_qver);
   warp_add(&io.stats->fp32_queries, n_q32);
+  if (lane == 0) {
+    atomicAdd(&io.stats->trip_cycles[0], cyc_pre);
+    atomicAdd(&io.stats->trip_cycles[1], cyc_search);
+    atomicAdd(&io.stats->trip_cycles[2], cyc_post);
+    atomicAdd(&io.stats->search_warp_steps, wsteps);
+    atomicAdd(&io.stats->search_lane_steps, lsteps);
+  }
 #endif
 }
 

@@ -159,6 +159,10 @@ struct DevStats {
   unsigned long long tie_deferred;     // rays waiting for the reference-order tree
   unsigned long long recheck_queries;  // guarded-FP32 queries with >= 1 FP64 re-check
   unsigned long long fp32_queries;     // guarded-FP32 split queries
+  // counters build: per-warp cycles before / in / after the split search of
+  // a loop trip, and search-loop steps of the warps and of all their lanes
+  unsigned long long trip_cycles[3];
+  unsigned long long search_warp_steps, search_lane_steps;
 };
 
 // Sum a small per-lane value over the active lanes, one atomic per warp.

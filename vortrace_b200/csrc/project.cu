@@ -215,6 +215,9 @@ static int finish_walk(vt_cloud* cl, WalkIO& io, const DevStats& hs, float ms, c
     stats->ties = hs.ties;
     stats->fp32_queries = hs.fp32_queries;
     stats->fp64_check_queries = hs.recheck_queries;
+    for (int i = 0; i < 3; ++i) stats->trip_cycles[i] = hs.trip_cycles[i];
+    stats->search_warp_steps = hs.search_warp_steps;
+    stats->search_lane_steps = hs.search_lane_steps;
   }
   if (hs.first_error != ~0ULL) {
     const int64_t ray = (int64_t)(hs.first_error >> 8);
@@ -327,18 +330,140 @@ __global__ void k_ray_keys(const double* __restrict__ S, const double* __restric
   idx[i] = (int32_t)i;
 }
 
-// Scratch of the ray sort for n rays: keys and indices (twice) and CUB's
-// temporary storage; 0 when the rays keep their order (few or too many).
-static int sort_rays_bytes(int64_t n, size_t& total, size_t& cub_bytes) {
-  total = cub_bytes = 0;
+// ------------------------------------------------ longest batches first
+// A warp walks 32 consecutive rays of the coherent order and takes the next
+// 32 only when all of them are done, so a launch ends when the warp that
+// drew the most expensive late batch ends.  Rays through dense regions cross
+// several times more cells than rays through the outskirts, and the coherent
+// order interleaves them, so with a few batches per warp (a 512x512 image:
+// 2.8 per resident warp) the last quarter of the launch runs a fraction of
+// the warps.  The batches are therefore handed out longest first (LPT
+// scheduling): each ray's cost is estimated by the number of device-tree
+// leaves whose tight box its segment crosses (an FP32 slab test per node,
+// a small fraction of the walk's own node visits), a batch costs its most
+// expensive ray, and the batches are sorted by decreasing cost class.  The
+// order only changes when each ray is walked, never what is computed.
+constexpr int kBatch = 32;
+
+__global__ void k_ray_cost(const double* __restrict__ S, const double* __restrict__ E,
+                           const int32_t* __restrict__ order, int64_t n, DevCloud c,
+                           uint32_t* __restrict__ cost) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t r = order[i];
+  float p0[3], inv[3];
+  bool ok = true;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const double a = S[3 * r + j] - c.origin[j], b = E[3 * r + j] - c.origin[j];
+    ok = ok && isfinite(a) && isfinite(b);
+    p0[j] = (float)a;
+    const float d = (float)(b - a);
+    inv[j] = d != 0.f ? 1.f / d : 1e30f;
+  }
+  uint32_t count = 0;
+  if (ok) {
+    const int64_t ninternal = c.nleaves - 1;
+    int64_t stack[kMaxDepth + 2];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+      const int64_t node = stack[--sp];
+      const float4 lo = __ldg(&c.boxlo[node]), hi = __ldg(&c.boxhi[node]);
+      // segment p0 + t (p1 - p0), t in [0, 1], against the box (slabs)
+      float t0 = 0.f, t1 = 1.f;
+      const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        float ta = (l[j] - p0[j]) * inv[j], tb = (h[j] - p0[j]) * inv[j];
+        if (ta > tb) {
+          const float t = ta;
+          ta = tb;
+          tb = t;
+        }
+        t0 = fmaxf(t0, ta);
+        t1 = fminf(t1, tb);
+      }
+      if (!(t0 <= t1)) continue;
+      if (node >= ninternal) {
+        ++count;
+      } else if (sp + 2 <= kMaxDepth + 2) {
+        stack[sp++] = 2 * node + 2;
+        stack[sp++] = 2 * node + 1;
+      }
+    }
+  }
+  cost[i] = count;
+}
+
+// Cost classes per doubling of the estimated cost: batches are sorted by
+// class (the radix sort is stable, so each class keeps the coherent order:
+// the warps running at the same time still share their region of the tree)
+#ifndef VT_LPT_CLASSES_PER_DOUBLING
+#define VT_LPT_CLASSES_PER_DOUBLING 1
+#endif
+// the reordering pays while each resident warp gets few batches; with many
+// (large images) the tail is short and the coherent order's cache sharing
+// between concurrent warps is worth more (measured on B200: +20% at 2.8
+// batches per warp, -1% at 11, -2% at 44)
+constexpr int kLptMaxBatchesPerWarp = 8;
+constexpr int kResidentWarpsPerSm = 20;  // the batched kernel: 5 blocks of 4 warps
+
+// key of batch b (ascending sort = decreasing cost class); the partial last
+// batch sorts last, so every other batch stays aligned to 32 queue slots
+__global__ void k_batch_keys(const uint32_t* __restrict__ cost, int64_t n, int64_t nb,
+                             uint32_t* __restrict__ keys, int32_t* __restrict__ idx) {
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const int64_t a = b * kBatch, e = a + kBatch < n ? a + kBatch : n;
+  uint32_t m = 0;
+  for (int64_t i = a; i < e; ++i) m = max(m, cost[i]);
+  const uint32_t cls = (uint32_t)(VT_LPT_CLASSES_PER_DOUBLING * log2f(1.0f + (float)m));
+  keys[b] = e - a < kBatch ? 0xffffffffu : ~min(cls, 0xfffffffeu);
+  idx[b] = (int32_t)b;
+}
+
+__global__ void k_permute_batches(const int32_t* __restrict__ order,
+                                  const int32_t* __restrict__ bsorted, int64_t n,
+                                  int32_t* __restrict__ out) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  out[k] = order[(int64_t)bsorted[k / kBatch] * kBatch + k % kBatch];
+}
+
+// Scratch of the ray sort for n rays: keys and indices (twice), the batch
+// costs, keys and indices (twice) and CUB's temporary storage of both
+// sorts; 0 when the rays keep their order (few or too many).
+struct SortLayout {
+  size_t kb, ib, nbb, cub_rays, cub_batches, total;
+};
+
+static size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static int sort_rays_layout(int64_t n, SortLayout& L) {
+  L = SortLayout{};
   if (n < 64 || n > (int64_t)0x7fffffff) return VT_OK;
-  VT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (unsigned long long*)nullptr,
+  const int64_t nb = (n + kBatch - 1) / kBatch;
+  VT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, L.cub_rays, (unsigned long long*)nullptr,
                                           (unsigned long long*)nullptr, (int32_t*)nullptr,
                                           (int32_t*)nullptr, (int)n, 0, 63));
-  const size_t kb = ((size_t)n * 8 + 255) & ~(size_t)255;
-  const size_t ib = ((size_t)n * 4 + 255) & ~(size_t)255;
-  total = 2 * kb + 2 * ib + cub_bytes;
+  VT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, L.cub_batches, (uint32_t*)nullptr,
+                                          (uint32_t*)nullptr, (int32_t*)nullptr,
+                                          (int32_t*)nullptr, (int)nb, 0, 32));
+  L.kb = up256((size_t)n * 8);
+  L.ib = up256((size_t)n * 4);
+  L.nbb = up256((size_t)nb * 4);
+  // keys x2 | idx x2 | cost | batch keys x2 | batch idx x2 | cub (max of both)
+  L.total = 2 * L.kb + 2 * L.ib + L.ib + 4 * L.nbb + std::max(L.cub_rays, L.cub_batches);
   return VT_OK;
+}
+
+static int sort_rays_bytes(int64_t n, size_t& total, size_t& cub_bytes) {
+  SortLayout L;
+  const int rc = sort_rays_layout(n, L);
+  total = L.total;
+  cub_bytes = L.cub_rays;
+  return rc;
 }
 
 // Enqueue the ray sort into `base` (sort_rays_bytes of scratch) and point
@@ -348,19 +473,45 @@ static int sort_rays_into(const DevCloud& view, WalkIO& io, uint8_t* base, size_
   const int64_t n = io.nrays;
   io.order = nullptr;
   if (total == 0) return VT_OK;
-  const size_t kb = ((size_t)n * 8 + 255) & ~(size_t)255;
-  const size_t ib = ((size_t)n * 4 + 255) & ~(size_t)255;
+  SortLayout L;
+  int rc = sort_rays_layout(n, L);
+  if (rc) return rc;
+  if (L.total > total) return set_error(VT_ERR_RUNTIME, "ray sort scratch too small");
+  const int64_t nb = (n + kBatch - 1) / kBatch;
   auto* k0 = reinterpret_cast<unsigned long long*>(base);
-  auto* k1 = reinterpret_cast<unsigned long long*>(base + kb);
-  auto* i0 = reinterpret_cast<int32_t*>(base + 2 * kb);
-  auto* i1 = reinterpret_cast<int32_t*>(base + 2 * kb + ib);
-  void* tmp = base + 2 * kb + 2 * ib;
+  auto* k1 = reinterpret_cast<unsigned long long*>(base + L.kb);
+  auto* i0 = reinterpret_cast<int32_t*>(base + 2 * L.kb);
+  auto* i1 = reinterpret_cast<int32_t*>(base + 2 * L.kb + L.ib);
+  auto* cost = reinterpret_cast<uint32_t*>(base + 2 * L.kb + 2 * L.ib);
+  uint8_t* bb = base + 2 * L.kb + 3 * L.ib;
+  auto* bk0 = reinterpret_cast<uint32_t*>(bb);
+  auto* bk1 = reinterpret_cast<uint32_t*>(bb + L.nbb);
+  auto* bi0 = reinterpret_cast<int32_t*>(bb + 2 * L.nbb);
+  auto* bi1 = reinterpret_cast<int32_t*>(bb + 3 * L.nbb);
+  void* tmp = bb + 4 * L.nbb;
   const int B = 256;
   k_ray_keys<<<(unsigned)((n + B - 1) / B), B, 0, st>>>(io.starts, io.ends, n, view, k0, i0);
   VT_CUDA(cudaGetLastError());
-  size_t cb = cub_bytes;
+  size_t cb = L.cub_rays;
   VT_CUDA(cub::DeviceRadixSort::SortPairs(tmp, cb, k0, k1, i0, i1, (int)n, 0, 63, st));
-  io.order = i1;
+  int dev = 0, nsms = 0;
+  VT_CUDA(cudaGetDevice(&dev));
+  VT_CUDA(cudaDeviceGetAttribute(&nsms, cudaDevAttrMultiProcessorCount, dev));
+  if (nb >= (int64_t)kLptMaxBatchesPerWarp * kResidentWarpsPerSm * nsms) {
+    io.order = i1;
+    return VT_OK;
+  }
+  // longest batches first: i1 (coherent order) -> i0 (batches by cost)
+  k_ray_cost<<<(unsigned)((n + B - 1) / B), B, 0, st>>>(io.starts, io.ends, i1, n, view, cost);
+  VT_CUDA(cudaGetLastError());
+  k_batch_keys<<<(unsigned)((nb + B - 1) / B), B, 0, st>>>(cost, n, nb, bk0, bi0);
+  VT_CUDA(cudaGetLastError());
+  cb = L.cub_batches;
+  VT_CUDA(cub::DeviceRadixSort::SortPairs(tmp, cb, bk0, bk1, bi0, bi1, (int)nb, 0, 32, st));
+  k_permute_batches<<<(unsigned)((n + B - 1) / B), B, 0, st>>>(i1, bi1, n, i0);
+  VT_CUDA(cudaGetLastError());
+  io.order = i0;
+  (void)cub_bytes;
   return VT_OK;
 }
 
