@@ -400,6 +400,14 @@ def measure(name, args, rank, world, dev, K, W, *, kp=None, wp=None, full=True,
     def rate(t_ms, steps):
         return tot_cross * steps / (t_ms / 1e3) / 1e6
 
+    def grad_sum():
+        # a loss over every rank's rays: each forward+adjoint step ends with
+        # the field gradient summed over the ranks on the device (one NCCL
+        # all-reduce of the N x nf FP64 gradient)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(d_grad, op=dist.ReduceOp.SUM)
+
     # --- autotune (outside the timed region): the AUTO kernel and the
     # shared-memory tree depth from timings on a sample of this workload's rays
     tune = pc.autotune(S, E, reduction={L.REDUCE_VOLUME: "volume"}.get(mode, "integrate"))
@@ -429,11 +437,11 @@ def measure(name, args, rank, world, dev, K, W, *, kp=None, wp=None, full=True,
 
     taped = mode in (L.REDUCE_SUM, L.REDUCE_VOLUME)
     # --- forward + adjoint: taped forward (AUTO) + scatter adjoint
-    t_fb = leg(lambda: (fwd_tape(L.KERNEL_AUTO), bwd_tape()), K, max(2, W // 2))
+    t_fb = leg(lambda: (fwd_tape(L.KERNEL_AUTO), bwd_tape(), grad_sum()), K, max(2, W // 2))
     fb_value = rate(t_fb, K)
     tape_entries = int(lib.vt_tape_size(tape.h))
     # --- forward + adjoint that re-walks the rays (no tape), AUTO kernel
-    t_rw = leg(lambda: (fwd(L.KERNEL_AUTO), bwd()), kp, wp)
+    t_rw = leg(lambda: (fwd(L.KERNEL_AUTO), bwd(), grad_sum()), kp, wp)
     rw_value = rate(t_rw, kp)
     # --- the batched kernel with the bounded FP64 k-NN
     t_f64 = leg(lambda: fwd(L.KERNEL_BATCHED_FP64), kp, wp)
@@ -445,11 +453,11 @@ def measure(name, args, rank, world, dev, K, W, *, kp=None, wp=None, full=True,
     img_plain = d_out.clone()
     # --- the plain kernel's forward + adjoint, like for like: taped plain
     # forward + the same scatter adjoint
-    t_ptb = leg(lambda: (fwd_tape(L.KERNEL_PLAIN_FP64), bwd_tape()), kp, wp)
+    t_ptb = leg(lambda: (fwd_tape(L.KERNEL_PLAIN_FP64), bwd_tape(), grad_sum()), kp, wp)
     ptb_value = rate(t_ptb, kp)
     # --- ... and with the plain kernel re-walking for the adjoint
     pc._cloud.set_param(L.PARAM_ADJOINT_KERNEL, L.KERNEL_PLAIN_FP64)
-    t_pfb = leg(lambda: (fwd(L.KERNEL_PLAIN_FP64), bwd()), kp, wp)
+    t_pfb = leg(lambda: (fwd(L.KERNEL_PLAIN_FP64), bwd(), grad_sum()), kp, wp)
     pc._cloud.set_param(L.PARAM_ADJOINT_KERNEL, L.KERNEL_AUTO)
     pfb_value = rate(t_pfb, kp)
 
@@ -464,6 +472,9 @@ def measure(name, args, rank, world, dev, K, W, *, kp=None, wp=None, full=True,
         "fwd_bwd_adjoint": (f"segment tape ({48 if mode == L.REDUCE_VOLUME else 16} "
                             "B/crossing) + scatter" if taped and tape_entries > 0
                             else "re-walk"),
+        "fwd_bwd_gradient_exchange": ("all-reduce (sum) of the N x nf FP64 field gradient "
+                                      f"over {world} ranks on the device (NCCL), every step"
+                                      if world > 1 else "none (1 rank)"),
         "fwd_bwd_rewalk_mcrossings_per_s": round(rw_value, 4),
         "bounded_fp64_mcrossings_per_s": round(f64_value, 4),
         "plain_fp64_mcrossings_per_s": round(pl_value, 4),

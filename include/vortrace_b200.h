@@ -247,6 +247,28 @@ int vt_project_grid(vt_cloud *cloud, const double extent[4], uint64_t nx, uint64
                     const double bounds[2], int mode, int kernel, double *out,
                     vt_stats *stats);
 
+/* One unrotated projection grid of a batch: the rays vt_grid_rays_device
+ * makes for extent = {x0, x1, y0, y1}, nx x ny pixels, z from bounds[0] to
+ * bounds[1]. */
+typedef struct {
+  double extent[4];
+  uint64_t nx, ny;
+  double bounds[2];
+} vt_grid_desc;
+/* Many projections in one walk launch.  Replaces the reference's one
+ * Projection / makeProjection per view (src/projection.cpp:26-73, driven by
+ * ProjectionCloud.grid_projection, vortrace/vortrace.py:141-195, once per
+ * grid): the rays of ngrids unrotated grids are generated on the device (as
+ * vt_grid_rays_device), followed by nrays arbitrary rays from host buffers
+ * (starts/ends nrays x 3; nrays may be 0 and the pointers NULL, e.g. rotated
+ * views generated on the host), all walked by one launch of `kernel`.  out
+ * holds (nx_0*ny_0 + ... + nrays) x nout values, grid by grid (ray i*ny + j
+ * of each), then the arbitrary rays in their order.  Errors as
+ * vt_project. */
+int vt_project_batch(vt_cloud *cloud, const vt_grid_desc *grids, uint64_t ngrids,
+                     const double *starts, const double *ends, uint64_t nrays, int mode,
+                     int kernel, double *out, vt_stats *stats);
+
 /* makeDetailedProjection + returnSegments (src/projection.cpp:75-144,
  * src/bindings.cpp:206-238).  Writes out (as vt_project) and the CSR
  * offsets (nrays + 1 entries), and returns a library-owned segment list

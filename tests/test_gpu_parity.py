@@ -229,6 +229,19 @@ def test_batch_projection_matches_individual(clustered):
         np.testing.assert_array_equal(img, pc.grid_projection(g["extent"], g["nres"],
                                                               g["bounds"], g["center"], **kw))
     np.testing.assert_array_equal(vals, pc.projection(rs, re_))
+    # a rotated grid first, two device grids after it, no arbitrary rays:
+    # the images come back in the order of the grids
+    grids2 = [grids[1], dict(extent=[48, 52], nres=(8, 12), bounds=[100, 0], center=None),
+              grids[0]]
+    imgs2 = pc.batch_projection(grids2)
+    # one launch for the whole batch
+    assert pc.last_stats["rays"] == 16 * 24 + 8 * 12 + 32 * 32
+    assert len(imgs2) == 3
+    for g, img in zip(grids2, imgs2):
+        kw = {k: v for k, v in g.items() if k not in ("extent", "nres", "bounds", "center")}
+        np.testing.assert_array_equal(img, pc.grid_projection(g["extent"], g["nres"],
+                                                              g["bounds"], g["center"], **kw))
+    assert imgs2[1].shape == (8, 12, 3)
 
 
 def test_neighbourhood_cache_is_exact(clustered):

@@ -49,8 +49,14 @@ EXPORTS = (
     "vt_tape_adjoint_device", "vt_slice", "vt_brute_projection", "vt_cloud_autotune",
     "vt_graph_create", "vt_graph_launch", "vt_graph_finish", "vt_graph_destroy",
     "vt_cloud_tree_save", "vt_cloud_tree_load", "vt_grid_rays_device", "vt_project_grid",
-    "vt_cloud_build_tie_tree",
+    "vt_cloud_build_tie_tree", "vt_project_batch",
 )
+
+
+class GridDesc(C.Structure):
+    """vt_grid_desc: one unrotated grid of a vt_project_batch call."""
+    _fields_ = [("extent", C.c_double * 4), ("nx", C.c_uint64), ("ny", C.c_uint64),
+                ("bounds", C.c_double * 2)]
 
 
 class CloudInfo(C.Structure):
@@ -177,6 +183,8 @@ def _open(p: str):
     L.vt_grid_rays_device.argtypes = [dp, u64, u64, dp, vp, vp, vp]
     L.vt_project_grid.argtypes = [vp, dp, u64, u64, dp, C.c_int, C.c_int, dp,
                                   C.POINTER(Stats)]
+    L.vt_project_batch.argtypes = [vp, vp, u64, dp, dp, u64, C.c_int, C.c_int, dp,
+                                   C.POINTER(Stats)]
     L.vt_tape_size.argtypes = [vp]
     L.vt_tape_size.restype = u64
     L.vt_project_device_tape.argtypes = [vp, vp, vp, vp, u64, C.c_int, C.c_int, vp, vp,
@@ -193,7 +201,7 @@ def _open(p: str):
                  "vt_slice", "vt_brute_projection", "vt_cloud_autotune",
                  "vt_graph_create", "vt_graph_launch", "vt_graph_finish",
                  "vt_cloud_tree_save", "vt_cloud_tree_load", "vt_grid_rays_device",
-                 "vt_project_grid"):
+                 "vt_project_grid", "vt_project_batch"):
         getattr(L, name).restype = C.c_int
     L.vt_set_warning_callback(_warn_cb)
     return L

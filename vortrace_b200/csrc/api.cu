@@ -567,6 +567,56 @@ int vt_project_grid(vt_cloud* cl, const double extent[4], uint64_t nx, uint64_t 
   VT_GUARD_END
 }
 
+int vt_project_batch(vt_cloud* cl, const vt_grid_desc* grids, uint64_t ngrids,
+                     const double* starts, const double* ends, uint64_t nrays, int mode,
+                     int kernel, double* out, vt_stats* stats) {
+  VT_GUARD_BEGIN
+  int rc = check_projectable(cl, mode);
+  if (rc) return rc;
+  if (ngrids > 0 && !grids) return set_error(VT_ERR_INVALID, "null argument");
+  if (nrays > 0 && (!starts || !ends)) return set_error(VT_ERR_INVALID, "null argument");
+  uint64_t total = nrays;
+  for (uint64_t g = 0; g < ngrids; ++g) {
+    if ((rc = check_grid_args(grids[g].extent, grids[g].nx, grids[g].ny, grids[g].bounds)))
+      return rc;
+    total += grids[g].nx * grids[g].ny;
+    if (total > (uint64_t)1 << 40) return set_error(VT_ERR_INVALID, "batch too large");
+  }
+  if (total > 0 && !out) return set_error(VT_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(cl->mu);
+  VT_CUDA(cudaSetDevice(cl->device));
+  if (stats) memset(stats, 0, sizeof(*stats));
+  if (total == 0) return VT_OK;
+  const int nout = mode == VT_REDUCE_VOLUME ? 3 : (int)cl->nfields;
+  if ((rc = cl->ws_starts.reserve(3 * total)) || (rc = cl->ws_ends.reserve(3 * total)) ||
+      (rc = cl->ws_out.reserve(total * nout)))
+    return rc;
+  cudaStream_t st = cl->stream;
+  // the grids' rays made on the device, one block of rays after another,
+  // then the arbitrary rays copied in behind them: one walk launch for all
+  uint64_t at = 0;
+  for (uint64_t g = 0; g < ngrids; ++g) {
+    if ((rc = vt::launch_grid_rays(grids[g].extent, grids[g].nx, grids[g].ny, grids[g].bounds,
+                                   cl->ws_starts.p + 3 * at, cl->ws_ends.p + 3 * at, st)))
+      return rc;
+    at += grids[g].nx * grids[g].ny;
+  }
+  if (nrays > 0) {
+    VT_CUDA(cudaMemcpyAsync(cl->ws_starts.p + 3 * at, starts, 3 * nrays * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+    VT_CUDA(cudaMemcpyAsync(cl->ws_ends.p + 3 * at, ends, 3 * nrays * sizeof(double),
+                            cudaMemcpyHostToDevice, st));
+  }
+  rc = project_device_locked(cl, cl->ws_starts.p, cl->ws_ends.p, total, mode, kernel,
+                             cl->ws_out.p, st, stats, vt::kOutImage, nullptr);
+  if (rc) return rc;
+  VT_CUDA(cudaMemcpyAsync(out, cl->ws_out.p, total * nout * sizeof(double),
+                          cudaMemcpyDeviceToHost, st));
+  VT_CUDA(cudaStreamSynchronize(st));
+  return VT_OK;
+  VT_GUARD_END
+}
+
 int vt_project_detailed(vt_cloud* cl, const double* starts, const double* ends, uint64_t nrays,
                         int mode, double* out, int64_t* offsets, vt_segments** segs) {
   VT_GUARD_BEGIN

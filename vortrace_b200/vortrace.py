@@ -394,28 +394,62 @@ class ProjectionCloud:
         images (one per grid) and, when ``rays`` is given, the ray values.
         """
         mode = self._validate_reduction(reduction)
-        starts, ends, shapes = [], [], []
-        for g in grids:
+        # unrotated grids: rays made on the device (vt_project_batch); the
+        # others (rotations, float32 extents) on the host, walked in the same
+        # launch behind them, then the arbitrary rays
+        descs, dev_idx, starts, ends, host_idx, shapes = [], [], [], [], [], []
+        for i, g in enumerate(grids):
+            args = None
+            if g.get("center") is None:
+                args = device_grid_args(g["extent"], g["nres"], g["bounds"], g.get("proj"))
+            if args is not None:
+                e4, nx, ny, b = args
+                d = L.GridDesc()
+                d.extent[:] = list(e4)
+                d.nx, d.ny = nx, ny
+                d.bounds[:] = list(b)
+                descs.append(d)
+                dev_idx.append(i)
+                shapes.append((nx, ny))
+                continue
             ps, pe = gr.generate_projection_grid(
                 g["extent"], g["nres"], g["bounds"], g.get("center"), proj=g.get("proj"),
                 yaw=g.get("yaw", 0.0), pitch=g.get("pitch", 0.0), roll=g.get("roll", 0.0))
             shapes.append(ps.shape[:-1])
             starts.append(ps.reshape(-1, 3))
             ends.append(pe.reshape(-1, 3))
+            host_idx.append(i)
+        nextra = 0
         if rays is not None:
             rs = self._prepare_array_for_backend(rays[0]).reshape(-1, 3)
             re_ = self._prepare_array_for_backend(rays[1]).reshape(-1, 3)
+            if rs.shape != re_.shape:
+                raise ValueError("pos_start / pos_end must have identical shapes")
             starts.append(rs)
             ends.append(re_)
+            nextra = rs.shape[0]
         S = np.ascontiguousarray(np.concatenate(starts)) if starts else np.empty((0, 3))
         E = np.ascontiguousarray(np.concatenate(ends)) if ends else np.empty((0, 3))
-        out = self._run(S, E, mode)
+        ndev = sum(int(d.nx * d.ny) for d in descs)
         nout = self._nout(mode)
-        imgs, o = [], 0
-        for sh in shapes:
+        if ndev + S.shape[0] == 0:
+            raise RuntimeError("Projection has not yet been made")
+        out = np.empty((ndev + S.shape[0], nout), np.float64)
+        st = L.Stats()
+        cl = self._cloud
+        arr = (L.GridDesc * max(1, len(descs)))(*descs)
+        L.check(cl._lib.vt_project_batch(cl._h, C.cast(arr, C.c_void_p), len(descs),
+                                         L.dptr(S) if S.shape[0] else None,
+                                         L.dptr(E) if E.shape[0] else None, S.shape[0], mode,
+                                         L.KERNELS[self.kernel], L.dptr(out), C.byref(st)))
+        self.last_stats = st.as_dict()
+        imgs = [None] * len(grids)
+        o = 0
+        for i in dev_idx + host_idx:  # the order of the rays in `out`
+            sh = shapes[i]
             k = int(np.prod(sh))
             blk = out[o:o + k]
-            imgs.append(blk.reshape(sh) if nout == 1 else blk.reshape(*sh, nout))
+            imgs[i] = blk.reshape(sh) if nout == 1 else blk.reshape(*sh, nout)
             o += k
         if rays is not None:
             return imgs, _as_values(out[o:], nout)
