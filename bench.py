@@ -252,11 +252,11 @@ def oracle_sample_parity(w, pc, kernel, nsample=4096):
             "values_max_rel_err_vs_oracle": float(rel.max()) if rel.size else 0.0}, idx, o
 
 
-def counters_run(w, kernel, smem_levels, mode):
+def counters_run(w, kernel, tune, mode):
     """One forward of the guarded-FP32 kernel through the library built
     with the search counters (libvortrace_b200_counters.so), outside the
-    timed region: nodes visited, FP64 re-checks and the queries that needed
-    one."""
+    timed region, on a tree and launch configured as the autotuner chose:
+    nodes visited, FP64 re-checks and the queries that needed one."""
     from vortrace_b200 import _lib as L
     from vortrace_b200 import build as B
     if not os.path.exists(B.LIB_COUNTERS):
@@ -272,8 +272,11 @@ def counters_run(w, kernel, smem_levels, mode):
         L.check(lib.vt_cloud_create(L.dptr(pos), pos.shape[0], L.dptr(f), pos.shape[0], nf,
                                     L.dptr(sb), None, 0, 0, C.byref(h)), lib)
     try:
+        L.check(lib.vt_cloud_set_param(h, L.PARAM_LEAF_SIZE, int(tune["leaf_size"])), lib)
         L.check(lib.vt_cloud_build_tree(h), lib)
-        L.check(lib.vt_cloud_set_param(h, L.PARAM_SMEM_LEVELS, int(smem_levels)), lib)
+        L.check(lib.vt_cloud_set_param(h, L.PARAM_SMEM_LEVELS, int(tune["smem_levels"])), lib)
+        L.check(lib.vt_cloud_set_param(h, L.PARAM_BLOCKS_PER_SM, int(tune["blocks_per_sm"])),
+                lib)
         S = np.ascontiguousarray(w["starts"])
         E = np.ascontiguousarray(w["ends"])
         n = S.shape[0]
@@ -408,9 +411,15 @@ def measure(name, args, rank, world, dev, K, W, *, kp=None, wp=None, full=True,
             import torch.distributed as dist
             dist.all_reduce(d_grad, op=dist.ReduceOp.SUM)
 
-    # --- autotune (outside the timed region): the AUTO kernel and the
-    # shared-memory tree depth from timings on a sample of this workload's rays
-    tune = pc.autotune(S, E, reduction={L.REDUCE_VOLUME: "volume"}.get(mode, "integrate"))
+    # --- autotune (outside the timed region): the AUTO kernel, the
+    # shared-memory tree depth, the resident blocks per SM and the leaf size
+    # from timings on a sample of this workload's rays
+    # (a sample of up to 2^20 rays: the whole 1024^2 image, a quarter of the
+    # 2048^2 one; leaf sizes are not tuned here: on a 262,144-ray sample of
+    # nested_16m leaf 6 with the FP64 search won, 5% slower than leaf 8 at
+    # full size)
+    tune = pc.autotune(S, E, reduction={L.REDUCE_VOLUME: "volume"}.get(mode, "integrate"),
+                       max_sample=min(n, 1 << 20))
     auto_kernel = tune["kernel"] if n >= tune["sample_rays"] else (
         "batched" if n < 65536 else "thread_fp32")
 
@@ -521,7 +530,7 @@ def measure(name, args, rank, world, dev, K, W, *, kp=None, wp=None, full=True,
             par["oracle_error"] = str(e)
         rec["parity"] = par
         try:
-            rec["counters"] = counters_run(w, L.KERNEL_THREAD_FP32, tune["smem_levels"], mode)
+            rec["counters"] = counters_run(w, L.KERNEL_THREAD_FP32, tune, mode)
         except Exception as e:
             rec["counters"] = {"error": str(e)}
 

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define VT_ABI_VERSION 1
+#define VT_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define VT_OK 0
@@ -81,6 +81,9 @@ extern "C" {
                                   /* (VT_KERNEL_*; default AUTO)               */
 #define VT_PARAM_DETAILED_KERNEL 10 /* walk kernel of vt_project_detailed      */
                                     /* (VT_KERNEL_*; default AUTO)             */
+#define VT_PARAM_TUNE_LEAF_SIZE 11  /* 1: vt_cloud_autotune also times leaf    */
+                                    /* sizes 6 and 12 (rebuilding the tree;    */
+                                    /* default 0)                              */
 
 typedef struct vt_cloud vt_cloud;
 typedef struct vt_segments vt_segments;
@@ -322,22 +325,34 @@ int vt_graph_launch(vt_graph *graph, void *stream);
 int vt_graph_finish(vt_graph *graph, void *stream, vt_stats *stats);
 void vt_graph_destroy(vt_graph *graph);
 
-/* Autotuner (no reference counterpart).  Times the walk kernels (one ray
- * per thread with the guarded-FP32 or the FP64 search, one ray per warp) and
- * the number of tree levels staged in shared memory (0-9) on a sample of
- * the given rays (host arrays, nrays x 3) -- up to max_sample (0: 262,144)
- * rays in four contiguous
- * blocks, each configuration run twice, the second run timed -- and makes
- * the fastest the cloud's VT_KERNEL_AUTO choice for batches at least as
- * large as the sample (VT_PARAM_SMEM_LEVELS is set to its value).  Results
- * of every kernel are the same bits; only the speed changes. */
+/* Autotuner (no reference counterpart).  On a sample of the given rays
+ * (host arrays, nrays x 3) -- up to max_sample (0: 262,144) rays in four
+ * contiguous blocks, each configuration run twice, the second run timed --
+ * it times, one dimension after the other:
+ *   1. the walk kernel (rays per warp: one ray per thread with the
+ *      guarded-FP32 or the FP64 search, or one ray per warp) x the tree
+ *      levels staged in shared memory (0-9);
+ *   2. for the chosen pair, the resident blocks per SM of the persistent
+ *      kernel (its occupancy: all that fit, 4 or 3 blocks of 128 threads);
+ *   3. with VT_PARAM_TUNE_LEAF_SIZE = 1, the tree's leaf size (the cloud's,
+ *      6 and 12; each candidate rebuilds the tree, ~30 ms per 2M points,
+ *      and the best one is kept, which invalidates graphs and tapes
+ *      recorded before);
+ * and makes the fastest the cloud's VT_KERNEL_AUTO choice for batches at
+ * least as large as the sample (VT_PARAM_SMEM_LEVELS, VT_PARAM_BLOCKS_PER_SM
+ * and VT_PARAM_LEAF_SIZE are set to its values).  The pending-point stack
+ * depth needs no tuning: rays whose stack outgrows the in-register one are
+ * finished by the global-stack kernel.  Results of every configuration are
+ * the same bits; only the speed changes. */
 typedef struct {
   int32_t kernel;           /* chosen VT_KERNEL_*                            */
   int32_t smem_levels;      /* chosen tree levels in shared memory           */
   int32_t tried;            /* configurations timed                          */
-  int32_t pad;
+  int32_t blocks_per_sm;    /* chosen resident blocks per SM (0: all fit)    */
   uint64_t sample_rays;     /* rays in the sample                            */
   double mcrossings_per_s;  /* the chosen configuration on the sample        */
+  int32_t leaf_size;        /* the tree's leaf size after tuning             */
+  int32_t pad;
 } vt_tune_result;
 int vt_cloud_autotune(vt_cloud *cloud, const double *starts, const double *ends,
                       uint64_t nrays, int mode, uint64_t max_sample,

@@ -28,11 +28,43 @@ def test_autotune_choice_keeps_results(case):
     ref = pc.projection(s, e)
     res = pc.autotune(s, e, max_sample=16384)
     assert res["kernel"] in ("thread_fp32", "batched_fp64", "batched")
-    assert res["tried"] == 8 and res["sample_rays"] == 16384 and res["mcrossings_per_s"] > 0
+    # 8 kernel x shared-memory depth pairs, then 2 occupancies
+    assert res["tried"] == 10 and res["sample_rays"] == 16384 and res["mcrossings_per_s"] > 0
+    assert res["blocks_per_sm"] in (0, 4, 3) and res["leaf_size"] == 8
     pc.kernel = "auto"
     np.testing.assert_array_equal(pc.projection(s, e), ref)
     with pytest.raises(ValueError):
         pc.autotune(s[:0], e[:0])
+
+
+def test_autotune_leaf_size_rebuilds_and_keeps_results(case):
+    pc, s, e = case
+    pc.kernel = "plain"
+    ref = pc.projection(s, e)
+    # a taped forward on the tree before tuning
+    import torch
+    from vortrace_b200 import autograd as ag
+    f = torch.tensor(pc.fields_orig.reshape(len(pc.pos_orig), -1), device="cuda",
+                     requires_grad=True)
+    img = ag.project(pc, f, s[:4096], e[:4096])
+    res = pc.autotune(s, e, max_sample=16384, leaf_size=True)
+    # three leaf sizes x (8 + 2) configurations
+    assert res["tried"] == 30 and res["leaf_size"] in (6, 8, 12)
+    info = pc._cloud.info()
+    assert info.tree_built
+    pc.kernel = "auto"
+    np.testing.assert_array_equal(pc.projection(s, e), ref)
+    # the tape recorded on the old tree is not used: the adjoint re-walks
+    img.sum().backward()
+    g_after = f.grad.clone()
+    f.grad = None
+    ag.project(pc, f, s[:4096], e[:4096]).sum().backward()
+    np.testing.assert_allclose(g_after.cpu().numpy(), f.grad.cpu().numpy(), rtol=1e-12,
+                               atol=1e-12 * float(f.grad.abs().max()))
+    # back to the default leaf size for the other tests of the module
+    pc._cloud.set_param(L.PARAM_LEAF_SIZE, 8)
+    pc._cloud.set_param(L.PARAM_TUNE_LEAF_SIZE, 0)
+    pc._cloud.buildTree()
 
 
 def test_adjoint_kernel_parameter(case):

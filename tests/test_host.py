@@ -30,7 +30,7 @@ def test_library_exports_header_symbols():
 
 def test_abi_and_verbose():
     lib = L.load()
-    assert lib.vt_abi_version() == 1
+    assert lib.vt_abi_version() == 2
     import vortrace_b200 as vt
     vt.set_verbose(True)
     assert vt.get_verbose() is True

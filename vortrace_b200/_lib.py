@@ -35,6 +35,7 @@ PARAM_LOCAL_STACK = 7
 PARAM_CACHE = 8
 PARAM_ADJOINT_KERNEL = 9
 PARAM_DETAILED_KERNEL = 10
+PARAM_TUNE_LEAF_SIZE = 11
 
 # every symbol the header declares (checked by the tests)
 EXPORTS = (
@@ -71,11 +72,14 @@ class CloudInfo(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("kernel", C.c_int32), ("smem_levels", C.c_int32), ("tried", C.c_int32),
-                ("pad", C.c_int32), ("sample_rays", C.c_uint64), ("mcrossings_per_s", C.c_double)]
+                ("blocks_per_sm", C.c_int32), ("sample_rays", C.c_uint64),
+                ("mcrossings_per_s", C.c_double), ("leaf_size", C.c_int32),
+                ("pad", C.c_int32)]
 
     def as_dict(self):
         names = {v: k for k, v in KERNELS.items()}
         return {"kernel": names.get(self.kernel, self.kernel), "smem_levels": self.smem_levels,
+                "blocks_per_sm": self.blocks_per_sm, "leaf_size": self.leaf_size,
                 "tried": self.tried, "sample_rays": self.sample_rays,
                 "mcrossings_per_s": self.mcrossings_per_s}
 

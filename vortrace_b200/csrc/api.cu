@@ -281,6 +281,7 @@ int vt_cloud_build_tree(vt_cloud* cl) {
   auto t1 = std::chrono::high_resolution_clock::now();
   cl->build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   cl->tree_built = true;
+  ++cl->tree_gen;
   if (vt::verbose())
     std::cout << "Tree build took " << (long long)cl->build_ms << " milliseconds." << std::endl;
   return VT_OK;
@@ -316,6 +317,7 @@ int vt_cloud_tree_load(vt_cloud* cl, const void* buf, uint64_t size) {
   auto t1 = std::chrono::high_resolution_clock::now();
   cl->build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   cl->tree_built = true;
+  ++cl->tree_gen;
   return VT_OK;
   VT_GUARD_END
 }
@@ -365,6 +367,10 @@ int vt_cloud_set_param(vt_cloud* cl, int param, int64_t value) {
     case VT_PARAM_LEAF_SIZE:
       if (value < 2 || value > 64) return set_error(VT_ERR_INVALID, "leaf size out of range [2, 64]");
       cl->leaf_size = (int)value;
+      return VT_OK;
+    case VT_PARAM_TUNE_LEAF_SIZE:
+      if (value < 0 || value > 1) return set_error(VT_ERR_INVALID, "tune leaf size must be 0 or 1");
+      cl->tune_leaf = (int)value;
       return VT_OK;
     default:
       return set_error(VT_ERR_INVALID, "unknown parameter " + std::to_string(param));
@@ -861,14 +867,12 @@ int vt_cloud_autotune(vt_cloud* cl, const double* starts, const double* ends, ui
                         {VT_KERNEL_THREAD_FP32, 5}, {VT_KERNEL_THREAD_FP32, 7},
                         {VT_KERNEL_THREAD_FP32, 9}, {VT_KERNEL_BATCHED_FP64, 0},
                         {VT_KERNEL_BATCHED_FP64, 5}, {VT_KERNEL_BATCHED, 5}};
-  const int saved_smem = cl->smem_levels;
-  double best_ms = -1.0;
-  Cand best = cands[0];
+  const int saved_smem = cl->smem_levels, saved_blocks = cl->blocks_per_sm;
   uint64_t crossings = 0;
-  for (const Cand& cd : cands) {
-    if (cl->periodic && cd.kernel != VT_KERNEL_THREAD_FP32) continue;  // one kernel serves them
-    cl->smem_levels = cd.smem;
-    double ms = 0.0;
+  // time one configuration (second of two runs); <0 on failure (rc set)
+  auto time_cfg = [&](int kernel, int smem, int blocks, double& ms_out) -> int {
+    cl->smem_levels = smem;
+    cl->blocks_per_sm = blocks;
     for (int rep = 0; rep < 2; ++rep) {  // the first run warms the caches
       vt::WalkIO io{};
       io.starts = ss.p;
@@ -877,26 +881,92 @@ int vt_cloud_autotune(vt_cloud* cl, const double* starts, const double* ends, ui
       io.nout = nout;
       io.out = so.p;
       vt_stats sts;
-      if ((rc = vt::run_walk(cl, io, vt::kOutImage, mode, cd.kernel, st, &sts))) {
-        cl->smem_levels = saved_smem;
-        return rc;
-      }
-      ms = sts.walk_ms;
+      const int r = vt::run_walk(cl, io, vt::kOutImage, mode, kernel, st, &sts);
+      if (r) return r;
+      ms_out = sts.walk_ms;
       crossings = sts.crossings;
     }
     ++result->tried;
-    if (best_ms < 0.0 || ms < best_ms) {
-      best_ms = ms;
-      best = cd;
+    return VT_OK;
+  };
+  struct Best {
+    int kernel, smem, blocks;
+    double ms;
+  } best{cands[0].kernel, cands[0].smem, 0, -1.0};
+  // 1. kernel (rays per warp) x shared-memory tree depth, all blocks that fit
+  auto tune_kernel = [&]() -> int {
+    best.ms = -1.0;
+    for (const Cand& cd : cands) {
+      if (cl->periodic && cd.kernel != VT_KERNEL_THREAD_FP32) continue;  // one kernel serves them
+      double ms = 0.0;
+      const int r = time_cfg(cd.kernel, cd.smem, 0, ms);
+      if (r) return r;
+      if (best.ms < 0.0 || ms < best.ms) best = Best{cd.kernel, cd.smem, 0, ms};
+    }
+    // 2. occupancy of the persistent kernel: fewer resident blocks leave
+    // each more L1
+    for (int blocks : {4, 3}) {
+      double ms = 0.0;
+      const int r = time_cfg(best.kernel, best.smem, blocks, ms);
+      if (r) return r;
+      if (ms < best.ms) best = Best{best.kernel, best.smem, blocks, ms};
+    }
+    return VT_OK;
+  };
+  auto restore = [&]() {
+    cl->smem_levels = saved_smem;
+    cl->blocks_per_sm = saved_blocks;
+  };
+  if ((rc = tune_kernel())) {
+    restore();
+    return rc;
+  }
+  // 3. leaf size (rebuilds the tree for each candidate; the results do not
+  // depend on it)
+  int best_leaf = cl->leaf_size;
+  if (cl->tune_leaf && !cl->periodic) {
+    const int leaf0 = cl->leaf_size;
+    const Best at0 = best;
+    auto rebuild = [&](int leaf) -> int {
+      cl->leaf_size = leaf;
+      cl->tree_built = false;
+      vt::drop_tie_tree(cl);
+      const int r = vt::build_tree_device(cl);
+      if (r) return r;
+      cl->tree_built = true;
+      ++cl->tree_gen;
+      return VT_OK;
+    };
+    Best overall = at0;
+    for (int leaf : {6, 12}) {
+      if (leaf == leaf0) continue;
+      if ((rc = rebuild(leaf)) || (rc = tune_kernel())) {
+        // leave the cloud as it was: its own leaf size and tree
+        restore();
+        rebuild(leaf0);
+        return rc;
+      }
+      if (best.ms < overall.ms) {
+        overall = best;
+        best_leaf = leaf;
+      }
+    }
+    best = overall;
+    if (cl->leaf_size != best_leaf && (rc = rebuild(best_leaf))) {
+      restore();
+      return rc;
     }
   }
   cl->smem_levels = best.smem;
+  cl->blocks_per_sm = best.blocks;
   cl->tuned_kernel = best.kernel;
   cl->tuned_min_rays = m;
   result->kernel = best.kernel;
   result->smem_levels = best.smem;
+  result->blocks_per_sm = best.blocks;
+  result->leaf_size = best_leaf;
   result->sample_rays = m;
-  result->mcrossings_per_s = best_ms > 0.0 ? (double)crossings / (best_ms * 1e3) : 0.0;
+  result->mcrossings_per_s = best.ms > 0.0 ? (double)crossings / (best.ms * 1e3) : 0.0;
   return VT_OK;
   VT_GUARD_END
 }
@@ -941,6 +1011,7 @@ int vt_project_device_tape(vt_cloud* cl, vt_tape* tape, const double* d_starts,
   tape->nfields = cl->nfields;
   tape->mode = mode;
   tape->cloud = cl;
+  tape->tree_gen = cl->tree_gen;
   const size_t esize = mode == VT_REDUCE_VOLUME ? sizeof(vt::TapeEntryV) : sizeof(vt::TapeEntry);
   if (nrays == 0) {
     tape->valid = true;
@@ -996,7 +1067,7 @@ int vt_tape_adjoint_device(vt_cloud* cl, vt_tape* tape, const double* d_starts,
   if (nrays == 0) return VT_OK;
   cudaStream_t st = pick_stream(cl, stream);
   if (tape->valid && tape->mode == mode && tape->cloud == cl && tape->nrays == nrays &&
-      tape->nfields == cl->nfields) {
+      tape->nfields == cl->nfields && tape->tree_gen == cl->tree_gen) {
     if (mode == VT_REDUCE_VOLUME)
       return vt::run_tape_scatter_vol(cl, tape->buf.p, tape->n, d_grad_out, d_out,
                                       d_grad_fields, st);

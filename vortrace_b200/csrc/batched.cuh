@@ -50,6 +50,12 @@ constexpr int kBatchStack = 32;
 #ifndef VT_BATCHED_COUNTERS
 #define VT_BATCHED_COUNTERS 0
 #endif
+#ifndef VT_I32_NODES
+#define VT_I32_NODES 0
+#endif
+#ifndef VT_I32_LEAF
+#define VT_I32_LEAF 0
+#endif
 
 // ---- node fetch (shared memory for the top levels) ----------------------
 struct Fetch64 {
@@ -65,6 +71,9 @@ struct Fetch32 {
   const float2* __restrict__ g;
   int nsm;
   __device__ __forceinline__ float2 operator()(int64_t i) const {
+    return i < nsm ? sm[i] : __ldg(&g[i]);
+  }
+  __device__ __forceinline__ float2 operator()(int i) const {
     return i < nsm ? sm[i] : __ldg(&g[i]);
   }
 };
@@ -210,7 +219,11 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
       off[d] = __fmul_rd(t, t);
     }
   }
+#if VT_I32_NODES
+  const int ninternal = (int)(c.nleaves - 1);
+#else
   const int64_t ninternal = c.nleaves - 1;
+#endif
   int node = 0;
   int sp = 0;
   int s_node[kMaxDepth + 2];
@@ -252,12 +265,24 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
       continue;
     }
     {
+#if VT_I32_LEAF
+      int a, b;
+      {
+        int64_t a64, b64;
+        leaf_range(c, node - ninternal, a64, b64);
+        a = (int)a64;
+        b = (int)b64;
+      }
+      typedef int LeafIdx;
+#else
       int64_t a, b;
       leaf_range(c, node - ninternal, a, b);
+      typedef int64_t LeafIdx;
+#endif
 #if VT_LEAF_BATCH
       // the FP32 distances of up to VT_LEAF_BATCH points first (independent
       // loads in flight together), then the tests in point order
-      for (int64_t p0 = a; p0 < b; p0 += VT_LEAF_BATCH) {
+      for (LeafIdx p0 = a; p0 < b; p0 += VT_LEAF_BATCH) {
         float fb[VT_LEAF_BATCH];
 #pragma unroll
         for (int j = 0; j < VT_LEAF_BATCH; ++j) {
@@ -266,7 +291,7 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
         }
 #pragma unroll
         for (int j = 0; j < VT_LEAF_BATCH; ++j) {
-        const int64_t p = p0 + j;
+        const LeafIdx p = p0 + j;
         const float f = fb[j];
 #else
       for (int64_t p = a; p < b; ++p) {

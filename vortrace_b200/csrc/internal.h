@@ -109,6 +109,8 @@ struct vt_cloud {
   int detailed_kernel = VT_KERNEL_AUTO;  // kernel of the detailed projection
   int tuned_kernel = VT_KERNEL_AUTO;    // vt_cloud_autotune's choice for AUTO
   uint64_t tuned_min_rays = 0;          // ... for batches at least this large
+  int tune_leaf = 0;                    // vt_cloud_autotune also tries leaf sizes
+  uint64_t tree_gen = 0;                // bumped by every tree build or load
   // device tree (tree order)
   vt::DevBuf<double4> pts_d;
   vt::DevBuf<float4> pts32_d;
@@ -152,6 +154,7 @@ struct vt_tape {
   uint64_t nfields = 0;
   int mode = 0;         // reduction of the last forward (SUM or VOLUME)
   const vt_cloud* cloud = nullptr;
+  uint64_t tree_gen = 0;  // the cloud's tree the entries refer to
   bool valid = false;   // the last forward recorded every segment
 };
 

@@ -462,10 +462,12 @@ class ProjectionCloud:
         return np.where(ids >= 0, self.orig_ids[np.maximum(ids, 0)], -1), r2
 
     def autotune(self, pos_start, pos_end, *, reduction="integrate",
-                 max_sample: int = 262144) -> dict:
-        """Time the walk kernels and shared-memory tree depths on a sample of
-        these rays (extension; not in the reference) and make the fastest
-        the ``'auto'`` kernel for batches at least as large as the sample.
+                 max_sample: int = 262144, leaf_size: bool = False) -> dict:
+        """Time the walk kernels (rays per warp), shared-memory tree depths and
+        resident blocks per SM on a sample of these rays (extension; not in
+        the reference) and make the fastest the ``'auto'`` configuration
+        for batches at least as large as the sample; with ``leaf_size`` the
+        tree is also rebuilt with leaf sizes 6 and 12 and the fastest kept.
         Results do not change, only the speed.  Returns the choice."""
         mode = self._validate_reduction(reduction)
         S = self._prepare_array_for_backend(pos_start).reshape(-1, 3)
@@ -473,6 +475,7 @@ class ProjectionCloud:
         if S.shape != E.shape:
             raise ValueError("pos_start / pos_end must have identical shapes")
         res = L.TuneResult()
+        self._cloud.set_param(L.PARAM_TUNE_LEAF_SIZE, 1 if leaf_size else 0)
         L.check(self._cloud._lib.vt_cloud_autotune(self._cloud._h, L.dptr(S), L.dptr(E),
                                                    S.shape[0], mode, int(max_sample),
                                                    C.byref(res)))
