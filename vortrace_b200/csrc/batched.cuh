@@ -50,12 +50,6 @@ constexpr int kBatchStack = 32;
 #ifndef VT_BATCHED_COUNTERS
 #define VT_BATCHED_COUNTERS 0
 #endif
-#ifndef VT_I32_NODES
-#define VT_I32_NODES 0
-#endif
-#ifndef VT_I32_LEAF
-#define VT_I32_LEAF 0
-#endif
 
 // ---- node fetch (shared memory for the top levels) ----------------------
 struct Fetch64 {
@@ -219,11 +213,9 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
       off[d] = __fmul_rd(t, t);
     }
   }
-#if VT_I32_NODES
+  // 32-bit node and point indices (the tree holds < 2^31 points): the
+  // 64-bit compares and address arithmetic cost 2% of the walk
   const int ninternal = (int)(c.nleaves - 1);
-#else
-  const int64_t ninternal = c.nleaves - 1;
-#endif
   int node = 0;
   int sp = 0;
   int s_node[kMaxDepth + 2];
@@ -265,7 +257,6 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
       continue;
     }
     {
-#if VT_I32_LEAF
       int a, b;
       {
         int64_t a64, b64;
@@ -274,11 +265,6 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
         b = (int)b64;
       }
       typedef int LeafIdx;
-#else
-      int64_t a, b;
-      leaf_range(c, node - ninternal, a, b);
-      typedef int64_t LeafIdx;
-#endif
 #if VT_LEAF_BATCH
       // the FP32 distances of up to VT_LEAF_BATCH points first (independent
       // loads in flight together), then the tests in point order
