@@ -286,3 +286,50 @@ def test_neighbourhood_cache_random_rays_and_segments(clustered):
     for a, b in zip(seg_on, seg_off):
         np.testing.assert_array_equal(np.asarray(a), np.asarray(b))
     np.testing.assert_array_equal(on, ot.project(S, E))
+
+
+def _segments_vs_oracle(pc, lp, ot, S, E, reduction, kernel):
+    """CSR segments (cells mapped to original ids, entry distances, lengths)
+    and values of the CUDA walk against the oracle's, on the same rays."""
+    oout, (ocid, ose, osx, ooff) = ot.project(S, E, reduction, segments=True)
+    pc.kernel = kernel
+    vals, cid, se, ds, off = pc.traced_projection(S, E, return_midpoint=False,
+                                                  reduction=reduction, flatten=True)
+    np.testing.assert_array_equal(off, ooff)
+    np.testing.assert_array_equal(cid, lp["orig_ids"][ocid])
+    np.testing.assert_array_equal(se, ose)
+    np.testing.assert_array_equal(ds, osx - ose)
+    return np.asarray(vals).reshape(len(S), -1), oout.reshape(len(S), -1)
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_clustered_2m_segments_vs_oracle(clustered, kernel):
+    """Segment-level parity on the benchmark cloud: an evenly spaced 2,048-ray
+    sample of the 1024x1024 image and of volume_2m's 512x512 image (the same
+    cloud), every kernel."""
+    w, pc, (lp, ot) = clustered
+    for starts, ends in ((w["starts"], w["ends"]), W.z_grid([40.0, 60.0], 512)):
+        idx = np.linspace(0, len(starts) - 1, 2048).astype(np.int64)
+        S, E = np.ascontiguousarray(starts[idx]), np.ascontiguousarray(ends[idx])
+        v, o = _segments_vs_oracle(pc, lp, ot, S, E, "integrate", kernel)
+        np.testing.assert_array_equal(v, o)
+
+
+@pytest.fixture(scope="module")
+def batched():
+    w = W.batched_1m()
+    return w, cloud(w["pos"], w["fields"], w["boundbox"]), oracle(w["pos"], w["fields"],
+                                                                  w["boundbox"])
+
+
+@pytest.mark.parametrize("kernel", ["thread_fp32", "batched_fp64"])
+def test_batched_1m_segments_vs_oracle(batched, kernel):
+    """Segment-level parity on batched_1m's rays: rotated views whose rays
+    start and end outside the cloud, and the 10,000 random rays."""
+    w, pc, (lp, ot) = batched
+    n = len(w["starts"])
+    idx = np.concatenate([np.linspace(0, n - 10_001, 3072).astype(np.int64),
+                          np.arange(n - 10_000, n - 10_000 + 1024)])
+    S, E = np.ascontiguousarray(w["starts"][idx]), np.ascontiguousarray(w["ends"][idx])
+    v, o = _segments_vs_oracle(pc, lp, ot, S, E, "integrate", kernel)
+    np.testing.assert_array_equal(v, o)
