@@ -414,7 +414,7 @@ int vt_cloud_get_info(const vt_cloud* cl, vt_cloud_info* info) {
   info->tree_build_ms = cl->build_ms;
   info->device_bytes = cl->pts_d.bytes() + cl->pts32_d.bytes() + cl->nodes_d.bytes() +
                        cl->nodes32_d.bytes() + cl->perm_d.bytes() + cl->fields_d.bytes() +
-                       cl->boxlo_d.bytes() + cl->boxhi_d.bytes() + cl->tt_nodes_d.bytes() +
+                       cl->boxlo_d.bytes() + cl->boxhi_d.bytes() + cl->leaf32_d.bytes() + cl->tt_nodes_d.bytes() +
                        cl->tt_pts_d.bytes() + cl->tt_tid_d.bytes();
   info->tie_tree_nodes = cl->view.tt_nodes ? cl->tt_nodes_d.n : 0;
   info->tie_tree_depth = cl->view.tt_nodes ? cl->tt_depth : 0;

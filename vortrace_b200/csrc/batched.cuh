@@ -33,10 +33,15 @@ constexpr int kBatchStack = 32;
 #ifndef VT_BATCHED_MINB
 #define VT_BATCHED_MINB 5
 #endif
-// points per batch of distances in a leaf scan of the FP32 / FP64 searches
-// (0: one at a time)
+// points per batch of distances in a leaf scan of the FP32 search (leaves
+// without SoA blocks) / of the FP64 search (0: one at a time)
 #ifndef VT_LEAF_BATCH
 #define VT_LEAF_BATCH 4
+#endif
+static_assert(VT_LEAF_BATCH > 0, "the FP32 leaf scan loads points in batches");
+// 1: the FP32 leaf scans read the SoA leaf blocks (DevCloud::leaf32)
+#ifndef VT_LEAF_SOA
+#define VT_LEAF_SOA 1
 #endif
 #ifndef VT_LEAF_BATCH64
 #define VT_LEAF_BATCH64 4
@@ -264,48 +269,56 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
         a = (int)a64;
         b = (int)b64;
       }
-      typedef int LeafIdx;
-#if VT_LEAF_BATCH
-      // the FP32 distances of up to VT_LEAF_BATCH points first (independent
-      // loads in flight together), then the tests in point order
-      for (LeafIdx p0 = a; p0 < b; p0 += VT_LEAF_BATCH) {
-        float fb[VT_LEAF_BATCH];
-#pragma unroll
-        for (int j = 0; j < VT_LEAF_BATCH; ++j) {
-          fb[j] = __int_as_float(0x7f800000);
-          if (p0 + j < b) fb[j] = pt_dist32(q0, q1, q2, __ldg(&c.pts32[p0 + j]));
-        }
-#pragma unroll
-        for (int j = 0; j < VT_LEAF_BATCH; ++j) {
-        const LeafIdx p = p0 + j;
-        const float f = fb[j];
-#else
-      for (int64_t p = a; p < b; ++p) {
-        const float4 P = __ldg(&c.pts32[p]);
-        const float d0 = __fsub_rn(q0, P.x), d1 = __fsub_rn(q1, P.y),
-                    d2 = __fsub_rn(q2, P.z);
-        const float f =
-            __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
-#endif
+      // a passing FP32 distance f of tree point p: FP64 re-check, insertion
+      auto test_point = [&](int p, float f) {
         if (f < thr32) {
-          const int pi = (int)p;
           double d;
-          if (pi == cid) d = dc;
-          else if (pi == nid) d = dn;
+          if (p == cid) d = dc;
+          else if (p == nid) d = dn;
           else {
             d = metric(qx, qy, qz, ldg_pt(&c.pts[p]));
             ++ver;
           }
           if (d < thr64) {
-            res.insert(d, pi);
+            res.insert(d, p);
             thr64 = fmin(R, res.worst());
             thr32 = __double2float_ru(dadd(thr64, G));
           }
         }
+      };
+      if (VT_LEAF_SOA && c.leaf32) {
+        // the leaf's SoA block: six independent 16-byte loads, three
+        // sectors; distances of all slots first, then the tests in point
+        // order (slots past the leaf's end hold +inf and never pass)
+        const float4* blk = c.leaf32 + (int64_t)(node - ninternal) * 6;
+        const float4 x0 = __ldg(blk), x1 = __ldg(blk + 1), y0 = __ldg(blk + 2),
+                     y1 = __ldg(blk + 3), z0 = __ldg(blk + 4), z1 = __ldg(blk + 5);
+        const float xs[kLeafSlots] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+        const float ys[kLeafSlots] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+        const float zs[kLeafSlots] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
+        float fb[kLeafSlots];
+#pragma unroll
+        for (int k = 0; k < kLeafSlots; ++k) {
+          const float e0 = __fsub_rn(q0, xs[k]), e1 = __fsub_rn(q1, ys[k]),
+                      e2 = __fsub_rn(q2, zs[k]);
+          fb[k] = __fadd_rn(__fadd_rn(__fmul_rn(e0, e0), __fmul_rn(e1, e1)), __fmul_rn(e2, e2));
+        }
+#pragma unroll
+        for (int k = 0; k < kLeafSlots; ++k) test_point(a + k, fb[k]);
+      } else {
+        // the FP32 distances of up to VT_LEAF_BATCH points first (independent
+        // loads in flight together), then the tests in point order
+        for (int p0 = a; p0 < b; p0 += VT_LEAF_BATCH) {
+          float fb[VT_LEAF_BATCH];
+#pragma unroll
+          for (int k = 0; k < VT_LEAF_BATCH; ++k) {
+            fb[k] = __int_as_float(0x7f800000);
+            if (p0 + k < b) fb[k] = pt_dist32(q0, q1, q2, __ldg(&c.pts32[p0 + k]));
+          }
+#pragma unroll
+          for (int k = 0; k < VT_LEAF_BATCH; ++k) test_point(p0 + k, fb[k]);
+        }
       }
-#if VT_LEAF_BATCH
-      }
-#endif
     }
     bool found = false;
     while (sp > 0) {

@@ -66,6 +66,8 @@ struct __align__(16) TieNode {
 };
 // deepest reference-order tree the tie-resolving search supports
 constexpr int kTieMaxDepth = 96;
+// points per SoA leaf block (DevCloud::leaf32)
+constexpr int kLeafSlots = 8;
 
 struct DevCloud {
   const double4* __restrict__ pts;
@@ -73,6 +75,10 @@ struct DevCloud {
   const double2* __restrict__ nodes;
   const float2* __restrict__ nodes32;
   const int32_t* __restrict__ perm;
+  // the pts32 values of each leaf as SoA blocks of kLeafSlots points
+  // (x[8], y[8], z[8]: 96 B, 3 sectors per leaf, +inf past the leaf's end)
+  // for the guarded-FP32 leaf scans; NULL when a leaf holds more points
+  const float4* __restrict__ leaf32;
   const double* __restrict__ fields;
   // tight FP32 boxes (of the pts32 values) of every heap node, internal
   // nodes first then leaves: node i in [0, 2L-1)

@@ -119,6 +119,7 @@ struct vt_cloud {
   vt::DevBuf<int32_t> perm_d;
   vt::DevBuf<double> fields_d;
   vt::DevBuf<float4> boxlo_d, boxhi_d;
+  vt::DevBuf<float4> leaf32_d;  // SoA leaf blocks (common.cuh)
   // reference-order tree (tietree.cu), built when an exact tie needs it
   vt::DevBuf<vt::TieNode> tt_nodes_d;
   vt::DevBuf<double4> tt_pts_d;

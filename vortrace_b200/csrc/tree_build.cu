@@ -242,6 +242,28 @@ __global__ void k_fields_tree(const double* __restrict__ f_in, const int32_t* __
 static inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // Tight boxes of the FP32 point copies: leaves from their points ...
+// SoA leaf blocks of the FP32 points: block j = 6 float4 {x[0..3], x[4..7],
+// y[0..3], y[4..7], z[0..3], z[4..7]} of leaf j, +inf past its end.
+__global__ void k_leaf_soa(const float4* __restrict__ pts32, int64_t n, int depth,
+                           int64_t nleaves, float4* __restrict__ out) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= nleaves) return;
+  const int64_t a = (j * n) >> depth, b = ((j + 1) * n) >> depth;
+  float v[3][kLeafSlots];
+  for (int k = 0; k < kLeafSlots; ++k) {
+    const bool in = a + k < b;
+    const float4 p = in ? pts32[a + k] : make_float4(0.f, 0.f, 0.f, 0.f);
+    v[0][k] = in ? p.x : INFINITY;
+    v[1][k] = in ? p.y : INFINITY;
+    v[2][k] = in ? p.z : INFINITY;
+  }
+  float4* o = out + j * 6;
+  for (int d = 0; d < 3; ++d) {
+    o[2 * d] = make_float4(v[d][0], v[d][1], v[d][2], v[d][3]);
+    o[2 * d + 1] = make_float4(v[d][4], v[d][5], v[d][6], v[d][7]);
+  }
+}
+
 __global__ void k_leaf_boxes(const float4* __restrict__ pts32, int64_t n, int depth,
                              int64_t nleaves, float4* lo, float4* hi) {
   int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -343,6 +365,12 @@ static int finish_tree(vt_cloud* cl, int depth, const double lo[3], const double
   VT_TRY(blo.alloc(2 * nleaves - 1));
   VT_TRY(bhi.alloc(2 * nleaves - 1));
   k_leaf_boxes<<<nblk(nleaves, B), B, 0, st>>>(pts32.p, n, depth, nleaves, blo.p, bhi.p);
+  // SoA leaf blocks when every leaf fits kLeafSlots points
+  DevBuf<float4> lsoa;
+  if (((n + nleaves - 1) >> depth) <= kLeafSlots) {
+    VT_TRY(lsoa.alloc(6 * nleaves));
+    k_leaf_soa<<<nblk(nleaves, B), B, 0, st>>>(pts32.p, n, depth, nleaves, lsoa.p);
+  }
   for (int l = depth - 1; l >= 0; --l)
     k_level_boxes<<<nblk(1LL << l, B), B, 0, st>>>(l, blo.p, bhi.p);
   {
@@ -367,6 +395,7 @@ static int finish_tree(vt_cloud* cl, int depth, const double lo[3], const double
   cl->fields_d = std::move(fields);
   cl->boxlo_d = std::move(blo);
   cl->boxhi_d = std::move(bhi);
+  cl->leaf32_d = std::move(lsoa);
   DevCloud& v = cl->view;
   v.pts = cl->pts_d.p;
   v.pts32 = cl->pts32_d.p;
@@ -376,6 +405,7 @@ static int finish_tree(vt_cloud* cl, int depth, const double lo[3], const double
   v.fields = cl->fields_d.p;
   v.boxlo = cl->boxlo_d.p;
   v.boxhi = cl->boxhi_d.p;
+  v.leaf32 = cl->leaf32_d.p;  // NULL when not built (leaves above kLeafSlots)
   v.n = n;
   v.nleaves = nleaves;
   v.nf = nf;
