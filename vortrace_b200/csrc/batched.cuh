@@ -29,9 +29,15 @@
 namespace vt {
 
 constexpr int kBatchStack = 32;
-// resident blocks per SM the batched kernel is compiled for (register cap)
+// resident blocks per SM the batched kernel is compiled for (register cap):
+// the guarded-FP32 search runs best at 5 blocks of 128 threads (96
+// registers), the FP64 one at 4 (128 registers: 818 against 768
+// Mcrossings/s on clustered_2m)
 #ifndef VT_BATCHED_MINB
 #define VT_BATCHED_MINB 5
+#endif
+#ifndef VT_BATCHED_MINB64
+#define VT_BATCHED_MINB64 4
 #endif
 // points per batch of distances in a leaf scan of the FP32 search (leaves
 // without SoA blocks) / of the FP64 search (0: one at a time)
@@ -39,6 +45,10 @@ constexpr int kBatchStack = 32;
 #define VT_LEAF_BATCH 4
 #endif
 static_assert(VT_LEAF_BATCH > 0, "the FP32 leaf scan loads points in batches");
+// 1: the SoA leaf scan re-checks its passing slots through a bit mask
+#ifndef VT_LEAF_MASK
+#define VT_LEAF_MASK 1
+#endif
 // 1: the FP32 leaf scans read the SoA leaf blocks (DevCloud::leaf32)
 #ifndef VT_LEAF_SOA
 #define VT_LEAF_SOA 1
@@ -287,24 +297,57 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
         }
       };
       if (VT_LEAF_SOA && c.leaf32) {
-        // the leaf's SoA block: six independent 16-byte loads, three
-        // sectors; distances of all slots first, then the tests in point
-        // order (slots past the leaf's end hold +inf and never pass)
-        const float4* blk = c.leaf32 + (int64_t)(node - ninternal) * 6;
-        const float4 x0 = __ldg(blk), x1 = __ldg(blk + 1), y0 = __ldg(blk + 2),
-                     y1 = __ldg(blk + 3), z0 = __ldg(blk + 4), z1 = __ldg(blk + 5);
-        const float xs[kLeafSlots] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-        const float ys[kLeafSlots] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
-        const float zs[kLeafSlots] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
+        // the leaf's SoA block: 3 * kLeafSlots / 4 independent 16-byte
+        // loads (8 slots: six loads, three sectors); distances of all slots
+        // first, then the tests in point order (slots past the leaf's end
+        // hold +inf and never pass)
+        constexpr int Q = kLeafSlots / 4;  // float4 per coordinate
+        const float4* blk = c.leaf32 + (int64_t)(node - ninternal) * (3 * Q);
+        float4 v[3 * Q];
+#pragma unroll
+        for (int u = 0; u < 3 * Q; ++u) v[u] = __ldg(blk + u);
         float fb[kLeafSlots];
 #pragma unroll
         for (int k = 0; k < kLeafSlots; ++k) {
-          const float e0 = __fsub_rn(q0, xs[k]), e1 = __fsub_rn(q1, ys[k]),
-                      e2 = __fsub_rn(q2, zs[k]);
+          const float4 X = v[k / 4], Y = v[Q + k / 4], Z = v[2 * Q + k / 4];
+          const int r = k & 3;
+          const float xk = r == 0 ? X.x : r == 1 ? X.y : r == 2 ? X.z : X.w;
+          const float yk = r == 0 ? Y.x : r == 1 ? Y.y : r == 2 ? Y.z : Y.w;
+          const float zk = r == 0 ? Z.x : r == 1 ? Z.y : r == 2 ? Z.z : Z.w;
+          const float e0 = __fsub_rn(q0, xk), e1 = __fsub_rn(q1, yk), e2 = __fsub_rn(q2, zk);
           fb[k] = __fadd_rn(__fadd_rn(__fmul_rn(e0, e0), __fmul_rn(e1, e1)), __fmul_rn(e2, e2));
         }
+#if VT_LEAF_MASK
+        // the slots under the threshold as a mask, then one FP64 re-check per
+        // set bit in slot order: lanes re-check their t-th passing point
+        // together.  A point that passed against the leaf's starting
+        // threshold but not against a threshold lowered by an insertion
+        // before it has f >= thr64 + G, hence d >= thr64, and the FP64 test
+        // rejects it, as the one-by-one scan would have skipped it.
+        unsigned pass = 0;
+#pragma unroll
+        for (int k = 0; k < kLeafSlots; ++k) pass |= (fb[k] < thr32 ? 1u : 0u) << k;
+        while (pass) {
+          const int k = __ffs(pass) - 1;
+          pass &= pass - 1;
+          const int p = a + k;
+          double d;
+          if (p == cid) d = dc;
+          else if (p == nid) d = dn;
+          else {
+            d = metric(qx, qy, qz, ldg_pt(&c.pts[p]));
+            ++ver;
+          }
+          if (d < thr64) {
+            res.insert(d, p);
+            thr64 = fmin(R, res.worst());
+            thr32 = __double2float_ru(dadd(thr64, G));
+          }
+        }
+#else
 #pragma unroll
         for (int k = 0; k < kLeafSlots; ++k) test_point(a + k, fb[k]);
+#endif
       } else {
         // the FP32 distances of up to VT_LEAF_BATCH points first (independent
         // loads in flight together), then the tests in point order
@@ -424,7 +467,8 @@ static __device__ __noinline__ RareOut rare_expand(const DevCloud& c, double x, 
 
 // --------------------------------------------------------------- kernel
 template <int MODE, int NF, int OUT, bool G32>
-__global__ void __launch_bounds__(128, VT_BATCHED_MINB) k_batched(DevCloud c, WalkIO io, int nsm) {
+__global__ void __launch_bounds__(128, G32 ? VT_BATCHED_MINB : VT_BATCHED_MINB64)
+    k_batched(DevCloud c, WalkIO io, int nsm) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // stage the top tree levels
   if (G32) {

@@ -67,7 +67,10 @@ struct __align__(16) TieNode {
 // deepest reference-order tree the tie-resolving search supports
 constexpr int kTieMaxDepth = 96;
 // points per SoA leaf block (DevCloud::leaf32)
-constexpr int kLeafSlots = 8;
+#ifndef VT_LEAF_SLOTS
+#define VT_LEAF_SLOTS 8
+#endif
+constexpr int kLeafSlots = VT_LEAF_SLOTS;
 
 struct DevCloud {
   const double4* __restrict__ pts;

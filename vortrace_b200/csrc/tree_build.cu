@@ -257,11 +257,11 @@ __global__ void k_leaf_soa(const float4* __restrict__ pts32, int64_t n, int dept
     v[1][k] = in ? p.y : INFINITY;
     v[2][k] = in ? p.z : INFINITY;
   }
-  float4* o = out + j * 6;
-  for (int d = 0; d < 3; ++d) {
-    o[2 * d] = make_float4(v[d][0], v[d][1], v[d][2], v[d][3]);
-    o[2 * d + 1] = make_float4(v[d][4], v[d][5], v[d][6], v[d][7]);
-  }
+  constexpr int Q = kLeafSlots / 4;  // float4 per coordinate
+  float4* o = out + j * 3 * Q;
+  for (int d = 0; d < 3; ++d)
+    for (int q = 0; q < Q; ++q)
+      o[Q * d + q] = make_float4(v[d][4 * q], v[d][4 * q + 1], v[d][4 * q + 2], v[d][4 * q + 3]);
 }
 
 __global__ void k_leaf_boxes(const float4* __restrict__ pts32, int64_t n, int depth,
@@ -368,7 +368,7 @@ static int finish_tree(vt_cloud* cl, int depth, const double lo[3], const double
   // SoA leaf blocks when every leaf fits kLeafSlots points
   DevBuf<float4> lsoa;
   if (((n + nleaves - 1) >> depth) <= kLeafSlots) {
-    VT_TRY(lsoa.alloc(6 * nleaves));
+    VT_TRY(lsoa.alloc((int64_t)(3 * kLeafSlots / 4) * nleaves));
     k_leaf_soa<<<nblk(nleaves, B), B, 0, st>>>(pts32.p, n, depth, nleaves, lsoa.p);
   }
   for (int l = depth - 1; l >= 0; --l)
