@@ -300,22 +300,30 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
         // the leaf's SoA block: 3 * kLeafSlots / 4 independent 16-byte
         // loads (8 slots: six loads, three sectors); distances of all slots
         // first, then the tests in point order (slots past the leaf's end
-        // hold +inf and never pass)
+        // hold -inf: their distance is +inf and never passes)
         constexpr int Q = kLeafSlots / 4;  // float4 per coordinate
         const float4* blk = c.leaf32 + (int64_t)(node - ninternal) * (3 * Q);
         float4 v[3 * Q];
 #pragma unroll
         for (int u = 0; u < 3 * Q; ++u) v[u] = __ldg(blk + u);
+        // distances two slots at a time with the packed FP32 operations of
+        // sm_100 (each half rounds as the scalar operation): e = q + (-p),
+        // f = ((ex^2 + ey^2) + ez^2), the order of pt_dist32
         float fb[kLeafSlots];
+        const float2 qx2 = make_float2(q0, q0), qy2 = make_float2(q1, q1),
+                     qz2 = make_float2(q2, q2);
 #pragma unroll
-        for (int k = 0; k < kLeafSlots; ++k) {
-          const float4 X = v[k / 4], Y = v[Q + k / 4], Z = v[2 * Q + k / 4];
-          const int r = k & 3;
-          const float xk = r == 0 ? X.x : r == 1 ? X.y : r == 2 ? X.z : X.w;
-          const float yk = r == 0 ? Y.x : r == 1 ? Y.y : r == 2 ? Y.z : Y.w;
-          const float zk = r == 0 ? Z.x : r == 1 ? Z.y : r == 2 ? Z.z : Z.w;
-          const float e0 = __fsub_rn(q0, xk), e1 = __fsub_rn(q1, yk), e2 = __fsub_rn(q2, zk);
-          fb[k] = __fadd_rn(__fadd_rn(__fmul_rn(e0, e0), __fmul_rn(e1, e1)), __fmul_rn(e2, e2));
+        for (int h = 0; h < kLeafSlots / 2; ++h) {
+          const float4 X = v[h / 2], Y = v[Q + h / 2], Z = v[2 * Q + h / 2];
+          const float2 px = (h & 1) ? make_float2(X.z, X.w) : make_float2(X.x, X.y);
+          const float2 py = (h & 1) ? make_float2(Y.z, Y.w) : make_float2(Y.x, Y.y);
+          const float2 pz = (h & 1) ? make_float2(Z.z, Z.w) : make_float2(Z.x, Z.y);
+          const float2 ex = __fadd2_rn(qx2, px), ey = __fadd2_rn(qy2, py),
+                       ez = __fadd2_rn(qz2, pz);
+          const float2 f2 = __fadd2_rn(__fadd2_rn(__fmul2_rn(ex, ex), __fmul2_rn(ey, ey)),
+                                       __fmul2_rn(ez, ez));
+          fb[2 * h] = f2.x;
+          fb[2 * h + 1] = f2.y;
         }
 #if VT_LEAF_MASK
         // the slots under the threshold as a mask, then one FP64 re-check per

@@ -78,9 +78,10 @@ struct DevCloud {
   const double2* __restrict__ nodes;
   const float2* __restrict__ nodes32;
   const int32_t* __restrict__ perm;
-  // the pts32 values of each leaf as SoA blocks of kLeafSlots points
-  // (x[8], y[8], z[8]: 96 B, 3 sectors per leaf, +inf past the leaf's end)
-  // for the guarded-FP32 leaf scans; NULL when a leaf holds more points
+  // the negated pts32 values of each leaf as SoA blocks of kLeafSlots
+  // points (-x[8], -y[8], -z[8]: 96 B, 3 sectors per leaf, -inf past the
+  // leaf's end) for the guarded-FP32 leaf scans, which form q - p as the
+  // packed sum q + (-p); NULL when a leaf holds more points
   const float4* __restrict__ leaf32;
   const double* __restrict__ fields;
   // tight FP32 boxes (of the pts32 values) of every heap node, internal

@@ -242,8 +242,9 @@ __global__ void k_fields_tree(const double* __restrict__ f_in, const int32_t* __
 static inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // Tight boxes of the FP32 point copies: leaves from their points ...
-// SoA leaf blocks of the FP32 points: block j = 6 float4 {x[0..3], x[4..7],
-// y[0..3], y[4..7], z[0..3], z[4..7]} of leaf j, +inf past its end.
+// SoA leaf blocks of the negated FP32 points: block j = 6 float4 {-x[0..3],
+// -x[4..7], -y[0..3], -y[4..7], -z[0..3], -z[4..7]} of leaf j, -inf past its
+// end (negation is exact, and q + (-p) rounds as q - p).
 __global__ void k_leaf_soa(const float4* __restrict__ pts32, int64_t n, int depth,
                            int64_t nleaves, float4* __restrict__ out) {
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -253,9 +254,9 @@ __global__ void k_leaf_soa(const float4* __restrict__ pts32, int64_t n, int dept
   for (int k = 0; k < kLeafSlots; ++k) {
     const bool in = a + k < b;
     const float4 p = in ? pts32[a + k] : make_float4(0.f, 0.f, 0.f, 0.f);
-    v[0][k] = in ? p.x : INFINITY;
-    v[1][k] = in ? p.y : INFINITY;
-    v[2][k] = in ? p.z : INFINITY;
+    v[0][k] = in ? -p.x : -INFINITY;
+    v[1][k] = in ? -p.y : -INFINITY;
+    v[2][k] = in ? -p.z : -INFINITY;
   }
   constexpr int Q = kLeafSlots / 4;  // float4 per coordinate
   float4* o = out + j * 3 * Q;
