@@ -45,6 +45,11 @@ constexpr int kBatchStack = 32;
 #define VT_LEAF_BATCH 4
 #endif
 static_assert(VT_LEAF_BATCH > 0, "the FP32 leaf scan loads points in batches");
+// 1: at a node just above the leaves both leaves are scanned in turn, the
+// farther one without a stack entry
+#ifndef VT_LEAF_PAIR
+#define VT_LEAF_PAIR 1
+#endif
 // 1: the SoA leaf scan re-checks its passing slots through a bit mask
 #ifndef VT_LEAF_MASK
 #define VT_LEAF_MASK 1
@@ -239,6 +244,11 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
   unsigned visits = 0, ver = 0;
   for (;;) {
     ++visits;
+    // the leaves to scan next: the current node if it is a leaf, or both
+    // children of a node just above the leaves (the nearer first, the other
+    // while its bound stays below the threshold: no stack entry for it)
+    int leaf0 = -1, leaf1 = -1;
+    float nm1 = 0.f;
     if (node < ninternal) {
       const float2 nd = fetch(node);
       const int first = 2 * node + 1;
@@ -260,22 +270,35 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
       const float o1 = dim == 1 ? fmaxf(t, off[1]) : off[1];
       const float o2 = dim == 2 ? fmaxf(t, off[2]) : off[2];
       const float nm = __fadd_rn(__fadd_rn(o0, o1), o2);
-      if (nm < thr32) {
-        s_node[sp] = other;
-        s_mind[sp] = nm;
-        s_off[sp][0] = o0;
-        s_off[sp][1] = o1;
-        s_off[sp][2] = o2;
-        ++sp;
+      if (VT_LEAF_PAIR && first >= ninternal) {
+        leaf0 = best - ninternal;
+        if (nm < thr32) {
+          leaf1 = other - ninternal;
+          nm1 = nm;
+        }
+      } else {
+        if (nm < thr32) {
+          s_node[sp] = other;
+          s_mind[sp] = nm;
+          s_off[sp][0] = o0;
+          s_off[sp][1] = o1;
+          s_off[sp][2] = o2;
+          ++sp;
+        }
+        node = best;
+        continue;
       }
-      node = best;
-      continue;
+    } else {
+      leaf0 = node - ninternal;
     }
-    {
+#pragma unroll 1
+    for (int lt = 0; lt < 2; ++lt) {
+      const int leaf = lt == 0 ? leaf0 : leaf1;
+      if (leaf < 0 || (lt == 1 && !(nm1 < thr32))) break;
       int a, b;
       {
         int64_t a64, b64;
-        leaf_range(c, node - ninternal, a64, b64);
+        leaf_range(c, leaf, a64, b64);
         a = (int)a64;
         b = (int)b64;
       }
@@ -302,7 +325,7 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
         // first, then the tests in point order (slots past the leaf's end
         // hold -inf: their distance is +inf and never passes)
         constexpr int Q = kLeafSlots / 4;  // float4 per coordinate
-        const float4* blk = c.leaf32 + (int64_t)(node - ninternal) * (3 * Q);
+        const float4* blk = c.leaf32 + (int64_t)leaf * (3 * Q);
         float4 v[3 * Q];
 #pragma unroll
         for (int u = 0; u < 3 * Q; ++u) v[u] = __ldg(blk + u);
