@@ -50,6 +50,10 @@ static_assert(VT_LEAF_BATCH > 0, "the FP32 leaf scan loads points in batches");
 #ifndef VT_LEAF_PAIR
 #define VT_LEAF_PAIR 1
 #endif
+// 1: the FP32 search keeps its newest stack entry in registers
+#ifndef VT_STACK_TOP
+#define VT_STACK_TOP 1
+#endif
 // 1: the SoA leaf scan re-checks its passing slots through a bit mask
 #ifndef VT_LEAF_MASK
 #define VT_LEAF_MASK 1
@@ -241,6 +245,13 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
   int s_node[kMaxDepth + 2];
   float s_off[kMaxDepth + 2][3];
   float s_mind[kMaxDepth + 2];
+#if VT_STACK_TOP
+  // the newest deferred subtree is kept in registers: a push followed by
+  // its pop (the far sibling after the near subtree) touches no local memory
+  bool tos = false;
+  int tos_node = 0;
+  float tos_mind = 0.f, tos_o0 = 0.f, tos_o1 = 0.f, tos_o2 = 0.f;
+#endif
   unsigned visits = 0, ver = 0;
   for (;;) {
     ++visits;
@@ -278,12 +289,29 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
         }
       } else {
         if (nm < thr32) {
+#if VT_STACK_TOP
+          if (tos) {
+            s_node[sp] = tos_node;
+            s_mind[sp] = tos_mind;
+            s_off[sp][0] = tos_o0;
+            s_off[sp][1] = tos_o1;
+            s_off[sp][2] = tos_o2;
+            ++sp;
+          }
+          tos = true;
+          tos_node = other;
+          tos_mind = nm;
+          tos_o0 = o0;
+          tos_o1 = o1;
+          tos_o2 = o2;
+#else
           s_node[sp] = other;
           s_mind[sp] = nm;
           s_off[sp][0] = o0;
           s_off[sp][1] = o1;
           s_off[sp][2] = o2;
           ++sp;
+#endif
         }
         node = best;
         continue;
@@ -395,6 +423,19 @@ __device__ __forceinline__ void knn3_guarded(const DevCloud& c, const F& fetch, 
       }
     }
     bool found = false;
+#if VT_STACK_TOP
+    if (tos) {
+      tos = false;
+      if (tos_mind < thr32) {
+        node = tos_node;
+        off[0] = tos_o0;
+        off[1] = tos_o1;
+        off[2] = tos_o2;
+        found = true;
+      }
+    }
+    if (!found)
+#endif
     while (sp > 0) {
       --sp;
       if (s_mind[sp] < thr32) {
