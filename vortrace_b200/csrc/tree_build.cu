@@ -363,9 +363,12 @@ static int finish_tree(vt_cloud* cl, int depth, const double lo[3], const double
   VT_TRY(fields.alloc((int64_t)n * nf));
   k_finalize<<<nblk(n, B), B, 0, st>>>(x, y, z, n, org[0], org[1], org[2], pts.p, pts32.p);
   DevBuf<float4> blo, bhi;
-  VT_TRY(blo.alloc(2 * nleaves - 1));
-  VT_TRY(bhi.alloc(2 * nleaves - 1));
-  k_leaf_boxes<<<nblk(nleaves, B), B, 0, st>>>(pts32.p, n, depth, nleaves, blo.p, bhi.p);
+  // one pad entry in front (as the node arrays): sibling boxes 2i+1, 2i+2
+  // share an aligned 32-byte sector
+  VT_TRY(blo.alloc(2 * nleaves));
+  VT_TRY(bhi.alloc(2 * nleaves));
+  k_leaf_boxes<<<nblk(nleaves, B), B, 0, st>>>(pts32.p, n, depth, nleaves, blo.p + 1,
+                                                bhi.p + 1);
   // SoA leaf blocks when every leaf fits kLeafSlots points
   DevBuf<float4> lsoa;
   if (((n + nleaves - 1) >> depth) <= kLeafSlots) {
@@ -373,7 +376,7 @@ static int finish_tree(vt_cloud* cl, int depth, const double lo[3], const double
     k_leaf_soa<<<nblk(nleaves, B), B, 0, st>>>(pts32.p, n, depth, nleaves, lsoa.p);
   }
   for (int l = depth - 1; l >= 0; --l)
-    k_level_boxes<<<nblk(1LL << l, B), B, 0, st>>>(l, blo.p, bhi.p);
+    k_level_boxes<<<nblk(1LL << l, B), B, 0, st>>>(l, blo.p + 1, bhi.p + 1);
   {
     // fields: upload in internal order into the (now free) aos buffer, gather
     DevBuf<double> fin;
@@ -404,8 +407,8 @@ static int finish_tree(vt_cloud* cl, int depth, const double lo[3], const double
   v.nodes32 = cl->nodes32_d.p + 1;  // after the pad entry
   v.perm = cl->perm_d.p;
   v.fields = cl->fields_d.p;
-  v.boxlo = cl->boxlo_d.p;
-  v.boxhi = cl->boxhi_d.p;
+  v.boxlo = cl->boxlo_d.p + 1;  // after the pad entry
+  v.boxhi = cl->boxhi_d.p + 1;
   v.leaf32 = cl->leaf32_d.p;  // NULL when not built (leaves above kLeafSlots)
   v.n = n;
   v.nleaves = nleaves;
