@@ -52,10 +52,10 @@ L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per crossing of
 # the walk kernel, from one single-pass ncu capture of the same launch
 # (clustered_2m, 1024x1024 rays, guarded-FP32 kernel with 3 tree levels in
-# shared memory, vortrace_b200.profile_walk: 1.541 GB read + 9.942 GB
+# shared memory, vortrace_b200.profile_walk: 0.849 GB read + 6.189 GB
 # written for 198,903,587 crossings), keyed by (workload, AUTO kernel); other
 # launches of the kernel are taken to scale with their crossings.
-DRAM_BYTES_PER_CROSSING = {("clustered_2m", "thread_fp32"): 57.73}
+DRAM_BYTES_PER_CROSSING = {("clustered_2m", "thread_fp32"): 35.38}
 
 
 def dist_env():
