@@ -87,7 +87,10 @@ int vt::check_projectable(const vt_cloud* cl, int mode) {
 // VT_KERNEL_AUTO: one ray per thread needs about 20 resident warps on each
 // of the device's SMs to hide its memory latency; batches smaller than
 // kThreadKernelMinRays cannot fill the device that way and run one ray per
-// warp instead (measured on B200: 16,384 rays, 1.4x faster per warp).
+// warp instead (measured on B200, contiguous blocks of the clustered_2m
+// image, Mcrossings/s one ray per warp / per thread: 1,024 rays 30 / 5,
+// 16,384 rays 126 / 97, 65,536 rays 142 / 324; short rays cross over
+// earlier: 16,384 rays of uniform_100k 174 / 188).
 // vt_cloud_autotune replaces the rule by its measured choice for batches of
 // at least its sample's size.
 constexpr uint64_t kThreadKernelMinRays = 65536;
