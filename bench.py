@@ -51,11 +51,14 @@ BX = {"clustered_2m": 3262.25, "uniform_100k": 2915.74, "volume_2m": 3273.36,
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per crossing of
 # the walk kernel, from one single-pass ncu capture of the same launch
-# (clustered_2m, 1024x1024 rays, guarded-FP32 kernel with 3 tree levels in
-# shared memory, vortrace_b200.profile_walk: 0.849 GB read + 6.189 GB
-# written for 198,903,587 crossings), keyed by (workload, AUTO kernel); other
-# launches of the kernel are taken to scale with their crossings.
-DRAM_BYTES_PER_CROSSING = {("clustered_2m", "thread_fp32"): 35.38}
+# (clustered_2m, 1024x1024 rays, guarded-FP32 kernel at 9 blocks per SM with
+# 3 tree levels in shared memory, vortrace_b200.profile_walk: 63.70 GB read
+# + 66.01 GB written for 198,903,587 crossings; the writes are local memory,
+# as the image is 25 MB: the spill and stack slots of 170K resident threads
+# outgrow the L2), keyed by
+# (workload, AUTO kernel); other launches of the kernel are taken to scale
+# with their crossings.
+DRAM_BYTES_PER_CROSSING = {("clustered_2m", "thread_fp32"): 652.15}
 
 
 def dist_env():

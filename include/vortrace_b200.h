@@ -326,14 +326,16 @@ int vt_graph_finish(vt_graph *graph, void *stream, vt_stats *stats);
 void vt_graph_destroy(vt_graph *graph);
 
 /* Autotuner (no reference counterpart).  On a sample of the given rays
- * (host arrays, nrays x 3) -- up to max_sample (0: 262,144) rays in four
+ * (host arrays, nrays x 3) -- up to max_sample (0: 1,048,576) rays in four
  * contiguous blocks, each configuration run twice, the second run timed --
  * it times, one dimension after the other:
  *   1. the walk kernel (rays per warp: one ray per thread with the
  *      guarded-FP32 or the FP64 search, or one ray per warp) x the tree
  *      levels staged in shared memory (0-9);
  *   2. for the chosen pair, the resident blocks per SM of the persistent
- *      kernel (its occupancy: all that fit, 4 or 3 blocks of 128 threads);
+ *      kernel (its occupancy: all that its register cap lets fit, 3/4 or
+ *      1/2 of them; a value above the cap of a later launch's kernel is
+ *      clamped to that cap);
  *   3. with VT_PARAM_TUNE_LEAF_SIZE = 1, the tree's leaf size (the cloud's,
  *      6 and 12; each candidate rebuilds the tree, ~30 ms per 2M points,
  *      and the best one is kept, which invalidates graphs and tapes

@@ -163,11 +163,16 @@ def test_tape_adjoint_matches_sparse_reference(sum_case, nf):
     dS = torch.as_tensor(s, device="cuda").contiguous()
     dE = torch.as_tensor(e, device="cuda").contiguous()
     sizes = []
-    for _ in range(3):
+    for it in range(3):
         img = _taped_forward(pc, tape, dS, dE)
         np.testing.assert_array_equal(img.cpu().numpy(), out)
         sizes.append(int(pc._cloud._lib.vt_tape_size(tape.h)))
-        np.testing.assert_allclose(_tape_adjoint(pc, tape, dS, dE, img, g), ref, **tol)
+        grad = _tape_adjoint(pc, tape, dS, dE, img, g)
+        bad = np.argwhere(~np.isclose(grad, ref, rtol=tol["rtol"], atol=tol["atol"]))
+        np.testing.assert_allclose(grad, ref, **tol, err_msg=(
+            f"forward {it} (tape size {sizes[-1]} of {nseg} segments), elements [cell, field] "
+            f"{bad[:8].tolist()}, got {grad[tuple(bad[:8].T)].tolist()}, "
+            f"want {ref[tuple(bad[:8].T)].tolist()}"))
     assert sizes[0] == 0 and sizes[1] == nseg and sizes[2] == nseg
     # rays deeper than one pending point are finished by the global-stack
     # kernel, which must not record their first segments twice

@@ -841,10 +841,11 @@ int vt_cloud_autotune(vt_cloud* cl, const double* starts, const double* ends, ui
   std::lock_guard<std::mutex> lk(cl->mu);
   VT_CUDA(cudaSetDevice(cl->device));
   if (nrays == 0) return set_error(VT_ERR_INVALID, "autotune needs at least one ray");
-  // the sample must fill the device several times over (148 SMs x 5 blocks
-  // x 128 threads ~ 95K rays resident), or it favours configurations that
-  // cope with low occupancy
-  if (max_sample == 0) max_sample = 262144;
+  // the sample must fill the device several times over (148 SMs x 9 blocks
+  // x 128 threads ~ 170K rays resident), or it favours configurations that
+  // cope with low occupancy; with 2^20 rays it also runs the guarded-FP32
+  // kernel at the register cap of large launches
+  if (max_sample == 0) max_sample = 1048576;
   const uint64_t m = nrays < max_sample ? nrays : max_sample;
   if (!starts || !ends) return set_error(VT_ERR_INVALID, "starts/ends must not be NULL");
   cudaStream_t st = cl->stream;
@@ -906,9 +907,11 @@ int vt_cloud_autotune(vt_cloud* cl, const double* starts, const double* ends, ui
       if (r) return r;
       if (best.ms < 0.0 || ms < best.ms) best = Best{cd.kernel, cd.smem, 0, ms};
     }
-    // 2. occupancy of the persistent kernel: fewer resident blocks leave
-    // each more L1
-    for (int blocks : {4, 3}) {
+    // 2. occupancy of the persistent kernel: fewer resident blocks than its
+    // launch bounds allow (3/4 and 1/2 of them) leave each more L1
+    const int full = vt::compiled_blocks_per_sm(best.kernel, (int64_t)m);
+    for (int blocks : {(3 * full) / 4, full / 2}) {
+      if (blocks < 1) blocks = 1;
       double ms = 0.0;
       const int r = time_cfg(best.kernel, best.smem, blocks, ms);
       if (r) return r;

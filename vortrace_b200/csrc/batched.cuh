@@ -29,12 +29,27 @@
 namespace vt {
 
 constexpr int kBatchStack = 32;
-// resident blocks per SM the batched kernel is compiled for (register cap):
-// the guarded-FP32 search runs best at 5 blocks of 128 threads (96
-// registers), the FP64 one at 4 (128 registers: 818 against 768
-// Mcrossings/s on clustered_2m)
+// resident blocks per SM the batched kernel is compiled for (register cap).
+// The guarded-FP32 search is compiled twice.  Launches with many rays per
+// resident thread run it at 9 blocks of 128 threads (56 registers): more
+// warps hide more of the dependent load latency than the extra spills cost
+// (clustered_2m, 1M rays, 5 / 7 / 8 / 9 / 10 / 12 blocks -> 1088 / 1131 /
+// 1150 / 1156 / 1060 / 427 Mcrossings/s; nested_16m, 4M rays, 1172 / 1278 /
+// 1327 / 1342 / 1240 / 460).  Launches with fewer rays than
+// VT_BATCHED_WIDE_RAYS_PER_THREAD per resident thread of that occupancy run
+// it at 5 blocks (96 registers): there each warp gets few batches, the
+// launch's tail dominates and the faster thread wins (volume_2m, 262,144
+// rays: 788 at 5 blocks, 674 at 9; uniform_100k, 16,384 rays: 180 / 171).
+// The FP64 search runs best at 4 blocks (128 registers: 822 against 768 /
+// 714 / 707 at 5 / 6 / 8 blocks on clustered_2m).
 #ifndef VT_BATCHED_MINB
-#define VT_BATCHED_MINB 5
+#define VT_BATCHED_MINB 9
+#endif
+#ifndef VT_BATCHED_MINB_FEW
+#define VT_BATCHED_MINB_FEW 5
+#endif
+#ifndef VT_BATCHED_WIDE_RAYS_PER_THREAD
+#define VT_BATCHED_WIDE_RAYS_PER_THREAD 3
 #endif
 #ifndef VT_BATCHED_MINB64
 #define VT_BATCHED_MINB64 4
@@ -538,9 +553,8 @@ static __device__ __noinline__ RareOut rare_expand(const DevCloud& c, double x, 
 }
 
 // --------------------------------------------------------------- kernel
-template <int MODE, int NF, int OUT, bool G32>
-__global__ void __launch_bounds__(128, G32 ? VT_BATCHED_MINB : VT_BATCHED_MINB64)
-    k_batched(DevCloud c, WalkIO io, int nsm) {
+template <int MODE, int NF, int OUT, bool G32, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_batched(DevCloud c, WalkIO io, int nsm) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // stage the top tree levels
   if (G32) {
@@ -862,6 +876,14 @@ __global__ void __launch_bounds__(128, G32 ? VT_BATCHED_MINB : VT_BATCHED_MINB64
 #endif
 }
 
+// The register cap of the guarded-FP32 kernel for a launch of nrays rays on
+// nsms SMs (see VT_BATCHED_MINB); the FP64 kernel has one.
+inline int batched_minb(bool g32, int64_t nrays, int nsms) {
+  if (!g32) return VT_BATCHED_MINB64;
+  const int64_t wide = (int64_t)VT_BATCHED_WIDE_RAYS_PER_THREAD * nsms * VT_BATCHED_MINB * 128;
+  return nrays >= wide ? VT_BATCHED_MINB : VT_BATCHED_MINB_FEW;
+}
+
 template <int MODE, int NF, int OUT>
 int launch_batched(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) {
   const bool g32 = kernel == VT_KERNEL_THREAD_FP32;
@@ -874,10 +896,15 @@ int launch_batched(vt_cloud* cl, WalkIO& io, int kernel, cudaStream_t st) {
   int dev = 0, nsms = 0;
   VT_CUDA(cudaGetDevice(&dev));
   VT_CUDA(cudaDeviceGetAttribute(&nsms, cudaDevAttrMultiProcessorCount, dev));
-  auto kfun = g32 ? k_batched<MODE, NF, OUT, true> : k_batched<MODE, NF, OUT, false>;
+  const int minb = batched_minb(g32, io.nrays, nsms);
+  auto kfun = !g32 ? k_batched<MODE, NF, OUT, false, VT_BATCHED_MINB64>
+              : minb == VT_BATCHED_MINB ? k_batched<MODE, NF, OUT, true, VT_BATCHED_MINB>
+                                        : k_batched<MODE, NF, OUT, true, VT_BATCHED_MINB_FEW>;
   if (smem > 48 * 1024)
     VT_CUDA(cudaFuncSetAttribute(kfun, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = cl->blocks_per_sm;
+  // a set (or tuned) occupancy above the kernel's register cap cannot be
+  // resident: clamp it
+  int per_sm = cl->blocks_per_sm < minb ? cl->blocks_per_sm : minb;
   if (per_sm <= 0) {
     VT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfun, B, smem));
     if (per_sm < 1) per_sm = 1;

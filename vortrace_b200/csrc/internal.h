@@ -174,6 +174,10 @@ int upload_fields(vt_cloud* cl, const double* src, bool src_device, cudaStream_t
 int check_projectable(const vt_cloud* cl, int mode);
 // the kernel VT_KERNEL_AUTO stands for with this cloud and batch size
 int resolve_kernel(const vt_cloud* cl, int kernel, uint64_t nrays);
+// resident blocks per SM the launch bounds of the walk kernel that runs a
+// launch of nrays rays are compiled for (VT_KERNEL_THREAD_FP32,
+// _BATCHED_FP64, _BATCHED on the current device; 0 for the others)
+int compiled_blocks_per_sm(int kernel, int64_t nrays);
 // pixel-centre z-grid rays on the device (grid.cu), ray i*ny + j
 int launch_grid_rays(const double extent[4], uint64_t nx, uint64_t ny, const double bounds[2],
                      double* d_starts, double* d_ends, cudaStream_t st);

@@ -402,12 +402,12 @@ __global__ void k_ray_cost(const double* __restrict__ S, const double* __restric
 #ifndef VT_LPT_CLASSES_PER_DOUBLING
 #define VT_LPT_CLASSES_PER_DOUBLING 1
 #endif
-// the reordering pays while each resident warp gets few batches; with many
-// (large images) the tail is short and the coherent order's cache sharing
-// between concurrent warps is worth more (measured on B200: +20% at 2.8
-// batches per warp, -1% at 11, -2% at 44)
-constexpr int kLptMaxBatchesPerWarp = 8;
-constexpr int kResidentWarpsPerSm = 20;  // the batched kernel: 5 blocks of 4 warps
+// the reordering pays while each SM gets few batches; with many (large
+// images) the tail is short and the coherent order's cache sharing between
+// concurrent warps is worth more (measured on B200 with 20 resident warps
+// per SM: +20% at 56 batches per SM, -1% at 221, -2% at 885; the threshold
+// is kept in batches per SM)
+constexpr int kLptMaxBatchesPerSm = 160;
 
 // key of batch b (ascending sort = decreasing cost class); the partial last
 // batch sorts last, so every other batch stays aligned to 32 queue slots
@@ -497,7 +497,7 @@ static int sort_rays_into(const DevCloud& view, WalkIO& io, uint8_t* base, size_
   int dev = 0, nsms = 0;
   VT_CUDA(cudaGetDevice(&dev));
   VT_CUDA(cudaDeviceGetAttribute(&nsms, cudaDevAttrMultiProcessorCount, dev));
-  if (nb >= (int64_t)kLptMaxBatchesPerWarp * kResidentWarpsPerSm * nsms) {
+  if (nb >= (int64_t)kLptMaxBatchesPerSm * nsms) {
     io.order = i1;
     return VT_OK;
   }
@@ -545,6 +545,24 @@ int run_walk(vt_cloud* cl, WalkIO& io, int out_kind, int mode, int kernel, cudaS
   io.gstack_cap = cl->stack_cap;
   io.slow_threads = slow_threads;
   return run_walk_on(cl, io, out_kind, mode, kernel, st, stats, nullptr, true);
+}
+
+int compiled_blocks_per_sm(int kernel, int64_t nrays) {
+  switch (kernel) {
+    case VT_KERNEL_THREAD_FP32: {
+      int dev = 0, nsms = 0;
+      if (cudaGetDevice(&dev) != cudaSuccess ||
+          cudaDeviceGetAttribute(&nsms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return VT_BATCHED_MINB_FEW;
+      return batched_minb(true, nrays, nsms);
+    }
+    case VT_KERNEL_BATCHED_FP64:
+      return VT_BATCHED_MINB64;
+    case VT_KERNEL_BATCHED:
+      return VT_WARP_MINB;
+    default:
+      return 0;
+  }
 }
 
 }  // namespace vt

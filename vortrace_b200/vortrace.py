@@ -462,7 +462,7 @@ class ProjectionCloud:
         return np.where(ids >= 0, self.orig_ids[np.maximum(ids, 0)], -1), r2
 
     def autotune(self, pos_start, pos_end, *, reduction="integrate",
-                 max_sample: int = 262144, leaf_size: bool = False) -> dict:
+                 max_sample: int = 1048576, leaf_size: bool = False) -> dict:
         """Time the walk kernels (rays per warp), shared-memory tree depths and
         resident blocks per SM on a sample of these rays (extension; not in
         the reference) and make the fastest the ``'auto'`` configuration
