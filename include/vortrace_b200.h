@@ -13,8 +13,10 @@
  *     reference's std::invalid_argument, i.e. Python ValueError) or another
  *     code (the reference's std::runtime_error, i.e. Python RuntimeError);
  *     the message is available from vt_last_error() on the calling thread;
- *   - a vt_cloud handle owns its device memory and one CUDA stream; calls on
- *     one handle are serialised by an internal mutex.
+ *   - a vt_cloud handle owns its device memory and one CUDA stream, a
+ *     blocking one: the work that a call given a NULL stream enqueues there
+ *     is ordered with the legacy default stream (stream 0) both ways; calls
+ *     on one handle are serialised by an internal mutex.
  */
 #ifndef VORTRACE_B200_H
 #define VORTRACE_B200_H

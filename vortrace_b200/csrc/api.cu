@@ -252,7 +252,12 @@ int vt_cloud_create(const double* pos, uint64_t npart, const double* fields,
   }
   if (cudaSetDevice(cl->device) != cudaSuccess)
     return set_error(VT_ERR_CUDA, "cannot select CUDA device " + std::to_string(cl->device));
-  VT_CUDA(cudaStreamCreateWithFlags(&cl->stream, cudaStreamNonBlocking));
+  // a blocking stream: a caller that passes NULL (for instance from the
+  // legacy default stream, PyTorch's default) gets its work ordered with that
+  // stream's, before and after, as if it had been enqueued there.  A
+  // non-blocking stream let an adjoint's atomics race the caller's zero fill
+  // of the gradient buffer and the caller's read of the result.
+  VT_CUDA(cudaStreamCreateWithFlags(&cl->stream, cudaStreamDefault));
   *out = cl.release();
   return VT_OK;
   VT_GUARD_END
