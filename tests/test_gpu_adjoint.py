@@ -186,6 +186,36 @@ def test_tape_adjoint_matches_sparse_reference(sum_case, nf):
         pc._cloud.set_param(L.PARAM_LOCAL_STACK, 1 << 30)
 
 
+def test_null_stream_adjoint_follows_the_default_stream(sum_case):
+    """A NULL stream selects the handle's stream, which is ordered with the
+    legacy default stream (PyTorch's default) both ways: a zero fill of the
+    gradient queued there behind a long kernel lands before the scatter adds
+    into the buffer, and a read there sees the finished scatter."""
+    import torch
+    pos, rho, s, e = sum_case
+    pc, lp, out, segs = setup(pos, rho, W.BOX, s, e, "integrate")
+    g = np.random.default_rng(7).normal(size=(len(s), 1))
+    ref = sparse_sum_gradient(segs, len(s), len(lp["orig_ids"]), g)
+    tape = L.Tape(pc._cloud._lib, pc._cloud._h)
+    dS = torch.as_tensor(s, device="cuda").contiguous()
+    dE = torch.as_tensor(e, device="cuda").contiguous()
+    assert torch.cuda.current_stream().cuda_stream == 0  # the legacy default stream
+    for _ in range(2):  # the second forward's tape fits (sized by the first)
+        img = _taped_forward(pc, tape, dS, dE)
+    assert int(pc._cloud._lib.vt_tape_size(tape.h)) == int(segs[3][-1])
+    gd = torch.as_tensor(np.ascontiguousarray(g), device="cuda")
+    grad = torch.full((len(pc.orig_ids), 1), 1e30, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    torch.cuda._sleep(100_000_000)  # about 50 ms of GPU time on the default stream
+    grad.zero_()                    # queued behind it
+    L.check(pc._cloud._lib.vt_tape_adjoint_device(pc._cloud._h, tape.h, dS.data_ptr(),
+                                                  dE.data_ptr(), dS.shape[0], L.REDUCE_SUM,
+                                                  img.data_ptr(), gd.data_ptr(), grad.data_ptr(),
+                                                  None))
+    np.testing.assert_allclose(grad.cpu().numpy(), ref, rtol=1e-12,
+                               atol=1e-14 * np.abs(ref).max())
+
+
 def test_tape_volume_adjoint(vol_case):
     """Volume forward with a tape (48 bytes per segment) gives the same image
     (1e-12) and its scatter adjoint matches the reverse-mode compositing
