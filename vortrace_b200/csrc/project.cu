@@ -699,13 +699,34 @@ void vt_graph_destroy(vt_graph* g) {
 
 namespace vt {
 
+// Block size of the tape scatters (one shared-memory slot per thread).
+constexpr int kScatterBlock = 256;
+
+// Sum of the terms v[] of the lanes in `peers` (ascending lane order, from
+// 0.0) through the warp's slots of shared memory: each lane stores its term,
+// the group's leader adds its peers' (a warp of shuffles per field cost
+// twice the time: 6.37 against 3.10 ms for clustered_2m's 1.99e8 entries).
+__device__ __forceinline__ double group_sum(double* s_warp, int lane, unsigned peers, bool leader,
+                                            double v) {
+  s_warp[lane] = v;
+  __syncwarp();
+  double sum = 0.0;
+  if (leader)
+    for (unsigned m = peers; m; m &= m - 1) sum += s_warp[__ffs(m) - 1];
+  __syncwarp();
+  return sum;
+}
+
 // Adjoint of 'integrate' from a tape: grad[pid, f] += gout[ray, f] * ds for
 // every entry.  The lanes of a warp holding the same cell add their terms
 // first (neighbouring rays cross the same cells), then one atomic per cell.
 template <int NF>
-__global__ void k_tape_scatter(const TapeEntry* __restrict__ t, uint64_t n, int nf_rt,
-                               const double* __restrict__ gout, double* __restrict__ grad) {
+__global__ void __launch_bounds__(kScatterBlock)
+    k_tape_scatter(const TapeEntry* __restrict__ t, uint64_t n, int nf_rt,
+                   const double* __restrict__ gout, double* __restrict__ grad) {
+  __shared__ double s_v[kScatterBlock];
   const int lane = threadIdx.x & 31;
+  double* s_warp = s_v + (threadIdx.x & ~31);
   const int nf = NF > 0 ? NF : nf_rt;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
@@ -722,12 +743,7 @@ __global__ void k_tape_scatter(const TapeEntry* __restrict__ t, uint64_t n, int 
     const bool leader = __ffs(peers) - 1 == lane;
     for (int f = 0; f < nf; ++f) {
       const double v = pid >= 0 ? gout[(int64_t)ray * nf + f] * ds : 0.0;
-      double sum = 0.0;
-#pragma unroll 8
-      for (int j = 0; j < 32; ++j) {
-        const double vj = __shfl_sync(0xffffffffu, v, j);
-        if ((peers >> j) & 1u) sum += vj;
-      }
+      const double sum = group_sum(s_warp, lane, peers, leader, v);
       if (leader && pid >= 0) atomicAdd(&grad[(int64_t)pid * nf + f], sum);
     }
   }
@@ -737,10 +753,13 @@ __global__ void k_tape_scatter(const TapeEntry* __restrict__ t, uint64_t n, int 
 // e = exp(-alpha ds), o = 1 - e, T and P of the entry and C the ray's final
 // colour, grad[rgb_k] += g_k T o and grad[alpha] += ds sum_k g_k (T rgb_k e -
 // (C_k - P_k)); lanes holding the same cell add their terms first.
-__global__ void k_tape_scatter_vol(DevCloud c, const TapeEntryV* __restrict__ t, uint64_t n,
-                                   const double* __restrict__ gout,
-                                   const double* __restrict__ fwd, double* __restrict__ grad) {
+__global__ void __launch_bounds__(kScatterBlock)
+    k_tape_scatter_vol(DevCloud c, const TapeEntryV* __restrict__ t, uint64_t n,
+                       const double* __restrict__ gout, const double* __restrict__ fwd,
+                       double* __restrict__ grad) {
+  __shared__ double s_v[kScatterBlock];
   const int lane = threadIdx.x & 31;
+  double* s_warp = s_v + (threadIdx.x & ~31);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
     const uint64_t i = base + threadIdx.x;
@@ -766,12 +785,7 @@ __global__ void k_tape_scatter_vol(DevCloud c, const TapeEntryV* __restrict__ t,
     const bool leader = __ffs(peers) - 1 == lane;
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-      double sum = 0.0;
-#pragma unroll 8
-      for (int j = 0; j < 32; ++j) {
-        const double vj = __shfl_sync(0xffffffffu, v[f], j);
-        if ((peers >> j) & 1u) sum += vj;
-      }
+      const double sum = group_sum(s_warp, lane, peers, leader, v[f]);
       if (leader && pid >= 0) atomicAdd(&grad[(int64_t)pid * 4 + f], sum);
     }
   }
@@ -783,7 +797,7 @@ int run_tape_scatter_vol(vt_cloud* cl, const void* tape, uint64_t n, const doubl
   int dev = 0, nsms = 0;
   VT_CUDA(cudaGetDevice(&dev));
   VT_CUDA(cudaDeviceGetAttribute(&nsms, cudaDevAttrMultiProcessorCount, dev));
-  const int B = 256;
+  const int B = kScatterBlock;
   uint64_t blocks = (n + B - 1) / B;
   if (blocks > (uint64_t)nsms * 16) blocks = (uint64_t)nsms * 16;
   k_tape_scatter_vol<<<(unsigned)blocks, B, 0, st>>>(
@@ -798,7 +812,7 @@ int run_tape_scatter(vt_cloud* cl, const void* tape, uint64_t n, const double* d
   int dev = 0, nsms = 0;
   VT_CUDA(cudaGetDevice(&dev));
   VT_CUDA(cudaDeviceGetAttribute(&nsms, cudaDevAttrMultiProcessorCount, dev));
-  const int B = 256;
+  const int B = kScatterBlock;
   uint64_t blocks = (n + B - 1) / B;
   if (blocks > (uint64_t)nsms * 16) blocks = (uint64_t)nsms * 16;
   const TapeEntry* t = static_cast<const TapeEntry*>(tape);
